@@ -1,0 +1,1132 @@
+// Device enumeration: one persistent, work-stealing kernel that counts
+// embeddings for one or many queries.
+//
+// Execution model.  Every warp is an independent depth-first searcher.  Work
+// items ("tasks") are prefixes of the search tree: for the candidate-table
+// mode the entries of E[order0][order1] (a root and one depth-1 extension),
+// for the cache mode the roots C(order0).  Tasks of all queries of a batch
+// form one index space; warps claim `grab` consecutive tasks with one atomic
+// on a global counter, so hub-rooted subtrees do not strand the rest of the
+// grid behind one warp.
+//
+// Warp state.  The search state of depth d lives in lane d % 32 (second
+// register set for depths 32..63): chosen candidate index and vertex, the
+// current list (pointer + length), the next batch position and the valid-mask
+// of the current 32-candidate batch.  Injectivity is a ballot over the lanes
+// holding the chosen vertices (explore.h:548's vis[] without a |V| array).
+//
+// Set intersection (common_ops.h:248-254 semantics: sorted uint32 lists, the
+// result keeps the shorter list's order) is warp-cooperative:
+//   * merge: the longer list is staged in shared memory, chunk by chunk, by a
+//     cp.async.bulk copy (16-byte aligned window, mbarrier completion with a
+//     bounded wait) or by plain loads; lanes binary-search the shorter list's
+//     elements in the staged chunk;
+//   * galloping: when the longer list exceeds a chunk and is more than
+//     gallop_ratio times longer, lanes binary-search it directly in global
+//     memory (L2-resident rows).
+// The last depth is never materialised: its count is |intersection| minus the
+// already-embedded vertices that fall in it (rank lookups + membership tests).
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "smx_internal.h"
+
+namespace smx {
+
+namespace {
+
+struct BnRef {
+    const uint32_t* off;   // candidate-table mode: E[bn][u] offsets
+    const uint32_t* edge;  // candidate-table mode: E[bn][u] candidate indices
+    uint32_t depth;        // depth of the backward neighbour
+    uint32_t max_deg;
+};
+
+struct DepthInfo {
+    const uint32_t* cand;  // C(u) (vertex ids, ascending)
+    uint32_t u;            // query vertex at this depth
+    uint32_t nbn;          // backward neighbours (explore.h: prevNeb[u].size())
+    uint32_t bn_begin;     // into QPlan::bn
+    uint32_t scr_off;      // this depth's list buffer in the warp scratch (elements)
+    uint64_t anc;          // DAF ancestor mask (prune.h:100-104)
+    uint32_t nops;         // cache mode: ops computed at this depth
+    uint32_t ops_begin;    // into QPlan::op
+    uint32_t iter_op;      // cache mode: op holding this depth's candidates
+    uint32_t pad;
+};
+
+struct OpInfo {
+    uint32_t parent;   // op id or kInvalid
+    uint32_t vdepth;   // conf_dep when this op comes out empty (explore.h:233)
+    uint32_t scr_off;  // result buffer in the warp scratch (elements)
+    uint32_t pad;
+};
+
+struct QPlan {
+    uint32_t n;          // query vertices
+    uint32_t qn;         // rank directory stride
+    uint32_t mode;       // smx_explore_kind
+    uint32_t nops;
+    uint64_t ntasks;
+    uint32_t nroot;      // |C(order0)|
+    uint32_t pad;
+    const uint2* rank;
+    const uint64_t* mask;
+    const uint64_t* off;    // data CSR
+    const uint32_t* adj;
+    const BnRef* bn;
+    const OpInfo* op;
+    DepthInfo dep[kMaxQ];
+};
+
+struct EnumArgs {
+    const QPlan* plans;
+    const uint64_t* task_prefix;    // nq + 1
+    unsigned long long* next_task;  // work queue head
+    unsigned long long* qcount;     // per query
+    uint32_t* qstop;                // per query: limit reached
+    const uint64_t* qlimit;         // per query, 0 = none
+    uint32_t* scratch;              // per warp lists
+    unsigned long long* stats;      // [0] intersections [1] nodes [2] bytes [3] tasks [4] pruned
+    int* status;                    // 0 ok, SMX_TIMEOUT, SMX_STOPPED, SMX_CUDA_ERROR
+    const volatile uint32_t* host_stop;
+    uint64_t scratch_stride;        // elements per warp
+    uint64_t budget_ns;             // time budget per warp from its start, 0 = none
+    uint32_t nq;
+    uint32_t max_ops;               // op-state entries per warp (cache mode)
+    uint32_t grab;
+    uint32_t chunk;                 // staged elements per warp
+    uint32_t gallop_ratio;
+    uint32_t use_tma;
+    uint32_t failing_sets;
+    uint32_t pad;
+};
+
+// ------------------------------------------------------------------ staging
+
+struct Stage {
+    uint32_t* buf;      // shared, 16-byte aligned, chunk + 8 elements
+    uint64_t* mbar;     // shared mbarrier (one arrival + tx bytes)
+    uint32_t phase;
+    uint32_t chunk;
+    bool tma;
+    bool failed;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Copies src[0, len) (len <= chunk) into the stage buffer; returns the index
+// of src[0] inside the buffer.  The bulk copy moves the 16-byte aligned
+// window that covers the row (at most 3 elements before and after it; every
+// list lives in an allocation padded by >= 32 bytes).
+__device__ uint32_t stage_load(Stage& s, const uint32_t* src, uint32_t len) {
+    const uint32_t lane = lane_id();
+    __syncwarp();
+    if (!s.tma || len < 64) {
+        for (uint32_t i = lane; i < len; i += 32) s.buf[i] = src[i];
+        __syncwarp();
+        return 0;
+    }
+#ifdef SMX_EMU
+    return 0;  // unreachable: the emulator runs with use_tma = 0
+#else
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const uintptr_t a0 = a & ~(uintptr_t)15;
+    const uint32_t head = (uint32_t)((a - a0) >> 2);
+    const uint32_t bytes = (uint32_t)(((a + (uintptr_t)len * 4 - a0) + 15) & ~(uintptr_t)15);
+    const uint32_t mb = smem_addr(s.mbar);
+    if (lane == 0) {
+        // order the warp's earlier generic-proxy accesses (reads of the stage
+        // buffer, writes of scratch lists that may be the source) before the
+        // async-proxy copy
+        asm volatile("fence.proxy.async;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_addr(s.buf)),
+            "l"(a0), "r"(bytes), "r"(mb)
+            : "memory");
+    }
+    // bounded wait on the phase
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < (1u << 24); ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(mb), "r"(s.phase)
+            : "memory");
+        if (done) break;
+    }
+    if (!__all_sync(kFull, done)) s.failed = true;
+    s.phase ^= 1u;
+    __syncwarp();
+    return head;
+#endif
+}
+
+// ------------------------------------------------------------------ intersection
+// Intersect sorted S[0, s) with sorted G[0, g), s <= g.  Writes the common
+// elements (in S order) to out unless COUNT_ONLY; returns the count.  out may
+// alias S (outputs never overtake the reads of the same batch).
+template <bool COUNT_ONLY>
+__device__ uint32_t isect(Stage& st, uint32_t gallop_ratio, const uint32_t* S, uint32_t s, const uint32_t* G,
+                          uint32_t g, uint32_t* out) {
+    const uint32_t lane = lane_id();
+    uint32_t cnt = 0;
+    if (s == 0 || g == 0) return 0;
+    if (g > st.chunk && (uint64_t)s * gallop_ratio < g) {
+        for (uint32_t base = 0; base < s; base += 32) {
+            const uint32_t i = base + lane;
+            bool f = false;
+            uint32_t x = 0;
+            if (i < s) {
+                x = S[i];
+                f = bsearch_global(G, g, x);
+            }
+            const uint32_t b = __ballot_sync(kFull, f);
+            if (!COUNT_ONLY && f) out[cnt + __popc(b & lanemask_lt())] = x;
+            cnt += __popc(b);
+        }
+        return cnt;
+    }
+    uint32_t sp = 0;
+    for (uint32_t cb = 0; cb < g && sp < s; cb += st.chunk) {
+        const uint32_t cl = min(st.chunk, g - cb);
+        const uint32_t glast = G[cb + cl - 1];
+        if (S[sp] > glast) continue;
+        const uint32_t head = stage_load(st, G + cb, cl);
+        const uint32_t* sh = st.buf + head;
+        const uint32_t se = (cb + cl >= g) ? s : sp + upper_bound_global(S + sp, s - sp, glast);
+        for (uint32_t base = sp; base < se; base += 32) {
+            const uint32_t i = base + lane;
+            bool f = false;
+            uint32_t x = 0;
+            if (i < se) {
+                x = S[i];
+                f = bsearch_shared(sh, cl, x);
+            }
+            const uint32_t b = __ballot_sync(kFull, f);
+            if (!COUNT_ONLY && f) out[cnt + __popc(b & lanemask_lt())] = x;
+            cnt += __popc(b);
+        }
+        sp = se;
+    }
+    __syncwarp();
+    return cnt;
+}
+
+// ------------------------------------------------------------------ lane-distributed slots
+#define SLOT_GET(f, d) __shfl_sync(kFull, ((d) < 32) ? f##0 : f##1, (d)&31)
+// The value is evaluated by every lane before the owning lane stores it, so
+// an argument that itself shuffles (SLOT_GET) never runs in one lane only.
+#define SLOT_SET(f, d, x)                                \
+    do {                                                 \
+        const auto slot_v_ = (x);                        \
+        if (lane == ((d)&31u)) {                         \
+            if ((d) < 32) f##0 = slot_v_; else f##1 = slot_v_; \
+        }                                                \
+    } while (0)
+
+struct Counters {
+    unsigned long long isect = 0, nodes = 0, bytes = 0, tasks = 0, pruned = 0;
+};
+
+// Flags that other warps (or the host) write are read by every lane; the
+// warp acts on the vote, so all lanes take the same branch even when the
+// write lands between the lanes' reads.
+__device__ __forceinline__ bool poll_abort(const EnumArgs& A) {
+    return __any_sync(kFull, *reinterpret_cast<volatile int*>(A.status) != 0);
+}
+
+__device__ __forceinline__ bool query_stopped(const EnumArgs& A, uint32_t q) {
+    return __any_sync(kFull, *reinterpret_cast<volatile uint32_t*>(A.qstop + q) != 0);
+}
+
+__device__ void check_global_stop(const EnumArgs& A, uint64_t deadline) {
+    if (lane_id() == 0) {
+        int code = 0;
+        if (A.host_stop && *A.host_stop) code = SMX_STOPPED;
+        else if (deadline && global_timer_ns() > deadline) code = SMX_TIMEOUT;
+        if (code) atomicCAS(A.status, 0, code);
+    }
+    __syncwarp();
+}
+
+// Per-task accumulation: flushed to the query's counter at task end and
+// whenever it grows large, so a limit stops long subtrees early.
+struct Tally {
+    unsigned long long local = 0;
+    uint32_t q = 0;
+};
+
+__device__ __forceinline__ void flush_tally(const EnumArgs& A, Tally& T) {
+    if (lane_id() == 0 && T.local) {
+        const unsigned long long tot = atomicAdd(A.qcount + T.q, T.local) + T.local;
+        if (A.qlimit[T.q] && tot >= A.qlimit[T.q]) atomicExch(A.qstop + T.q, 1u);
+    }
+    T.local = 0;
+    __syncwarp();
+}
+
+// Periodic in-task check: abort flag, the query's limit, large local tallies.
+__device__ __forceinline__ bool task_should_stop(const EnumArgs& A, Tally& T) {
+    if (T.local > (1ull << 22)) flush_tally(A, T);
+    const bool a = poll_abort(A);
+    const bool b = query_stopped(A, T.q);
+    return a || b;
+}
+
+// ================================================================== candidate-table mode
+struct Row {
+    const uint32_t* p;
+    uint32_t len;
+};
+
+__device__ __forceinline__ Row table_row(const BnRef& r, uint32_t idx) {
+    const uint32_t s = __ldg(r.off + idx);
+    return Row{r.edge + s, __ldg(r.off + idx + 1) - s};
+}
+
+// Candidate list of depth D (CandidatesBuffer::getNextCandidatesImpl,
+// explore.h:284-354): with one backward neighbour the table row itself (no
+// copy), otherwise the intersection of all rows, shortest first, in the
+// depth's scratch buffer.  For the last depth (COUNT_ONLY) returns
+// |intersection| and leaves the two lists that define it in r0 / r1 for the
+// conflict test.
+template <bool COUNT_ONLY>
+__device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr, Stage& st, uint32_t gallop_ratio,
+                               Counters& C, Row& r0, Row& r1, const uint32_t (&slot_idx)[2]) {
+    const uint32_t lane = lane_id();
+    const uint32_t nb = D.nbn;
+    // lane i < min(nb, 32) holds row i
+    Row mine{nullptr, 0xffffffffu};
+    {
+        uint32_t bd = 0;
+        BnRef R{};
+        if (lane < nb) {
+            R = P.bn[D.bn_begin + lane];
+            bd = R.depth;
+        }
+        const uint32_t id_lo = __shfl_sync(kFull, slot_idx[0], bd & 31);
+        const uint32_t id_hi = __shfl_sync(kFull, slot_idx[1], bd & 31);
+        if (lane < nb) mine = table_row(R, bd < 32 ? id_lo : id_hi);
+    }
+    if (nb == 1) {
+        r0 = Row{reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(mine.p), 0)),
+                 __shfl_sync(kFull, mine.len, 0)};
+        r1 = Row{nullptr, 0};
+        return r0.len;
+    }
+    // order rows by length: repeatedly take the shortest unused one
+    uint32_t used = 0;  // bit per lane
+    auto take_shortest = [&](Row& out) {
+        const bool avail = lane < nb && !((used >> lane) & 1u);
+        const uint32_t key = avail ? mine.len : 0xffffffffu;
+        const uint32_t mn = __reduce_min_sync(kFull, key);
+        const uint32_t who = __ffs(__ballot_sync(kFull, avail && key == mn)) - 1;
+        used |= 1u << who;
+        out.p = reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(mine.p), who));
+        out.len = __shfl_sync(kFull, mine.len, who);
+    };
+    const uint32_t nrows = min(nb, 32u);
+    Row a, b;
+    take_shortest(a);
+    take_shortest(b);
+    C.isect++;
+    C.bytes += 4ull * (a.len + b.len);
+    if (nrows == 2 && nb <= 32) {
+        if (COUNT_ONLY) {
+            r0 = a;
+            r1 = b;
+            return isect<true>(st, gallop_ratio, a.p, a.len, b.p, b.len, nullptr);
+        }
+        const uint32_t k = isect<false>(st, gallop_ratio, a.p, a.len, b.p, b.len, scr);
+        r0 = Row{scr, k};
+        r1 = Row{nullptr, 0};
+        return k;
+    }
+    // three or more rows: materialise all but the longest, then count with it
+    uint32_t k = isect<false>(st, gallop_ratio, a.p, a.len, b.p, b.len, scr);
+    for (uint32_t t = 2; t < nrows; ++t) {
+        Row c;
+        take_shortest(c);
+        if (k == 0) {
+            r0 = Row{scr, 0};
+            r1 = Row{nullptr, 0};
+            return 0;
+        }
+        C.isect++;
+        C.bytes += 4ull * (k + c.len);
+        const bool last = (t + 1 == nrows) && nb <= 32;
+        if (last && COUNT_ONLY) {
+            r0 = Row{scr, k};
+            r1 = c;
+            return isect<true>(st, gallop_ratio, scr, k, c.p, c.len, nullptr);
+        }
+        // k <= every row taken so far <= c.len: scr stays the shorter side (in place is safe)
+        k = isect<false>(st, gallop_ratio, scr, k, c.p, c.len, scr);
+    }
+    // backward neighbours beyond 32 (queries with more than 33 vertices): in input order
+    for (uint32_t i = 32; i < nb; ++i) {
+        const BnRef R = P.bn[D.bn_begin + i];
+        const uint32_t id = __shfl_sync(kFull, R.depth < 32 ? slot_idx[0] : slot_idx[1], R.depth & 31);
+        const Row c = table_row(R, id);
+        if (k == 0) break;
+        C.isect++;
+        C.bytes += 4ull * (k + c.len);
+        if (k <= c.len) {
+            k = isect<false>(st, gallop_ratio, scr, k, c.p, c.len, scr);
+        } else {
+            // the row is the shorter side: the output would overtake reads of scr,
+            // so write it past scr's current contents first, then move it down
+            const uint32_t k2 = isect<false>(st, gallop_ratio, c.p, c.len, scr, k, scr + k);
+            for (uint32_t j = lane; j < k2; j += 32) scr[j] = scr[k + j];
+            __syncwarp();
+            k = k2;
+        }
+    }
+    r0 = Row{scr, k};
+    r1 = Row{nullptr, 0};
+    return k;
+}
+
+// Full-warp count of the last depth L for the current prefix (depths < L set).
+__device__ uint64_t last_depth_count(const QPlan& P, uint32_t L, uint32_t* scr_base, Stage& st,
+                                     uint32_t gallop_ratio, Counters& C, const uint32_t (&slot_idx)[2],
+                                     const uint32_t (&slot_vid)[2]) {
+    const uint32_t lane = lane_id();
+    const DepthInfo& D = P.dep[L];
+    Row r0, r1;
+    const uint32_t k = build_rows<true>(P, D, scr_base + D.scr_off, st, gallop_ratio, C, r0, r1, slot_idx);
+    if (k == 0) return 0;
+    // embedded vertices that are candidates of u_L and lie in the result
+    uint32_t conflicts = 0;
+    for (uint32_t half = 0; half < 2; ++half) {
+        const uint32_t j = half * 32 + lane;
+        bool in = false;
+        if (j < L) {
+            const uint32_t v = half ? slot_vid[1] : slot_vid[0];
+            if ((__ldg(P.mask + v) >> D.u) & 1ull) {
+                const uint32_t r = cand_rank(P.rank, P.qn, D.u, v);
+                in = bsearch_global(r0.p, r0.len, r) && (r1.p == nullptr || bsearch_global(r1.p, r1.len, r));
+            }
+        }
+        conflicts += __popc(__ballot_sync(kFull, in));
+        if (L <= 32) break;
+    }
+    return (uint64_t)(k - conflicts);
+}
+
+// One task: root r = row of entry t in E[o0][o1], depth-1 candidate edge[t].
+__device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, Stage& st, Counters& C,
+                               Tally& T) {
+    unsigned long long& local = T.local;
+    const uint32_t lane = lane_id();
+    const uint32_t n = P.n;
+    const DepthInfo& D0 = P.dep[0];
+    const DepthInfo& D1 = P.dep[1];
+    const BnRef R01 = P.bn[D1.bn_begin];
+    // root index: last r with off[r] <= t (off has |C(o0)| + 1 entries)
+    uint32_t lo = 0, hi = P.nroot;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((uint64_t)__ldg(R01.off + mid) <= t) lo = mid; else hi = mid;
+    }
+    const uint32_t r = lo;
+    const uint32_t c1 = __ldg(R01.edge + t);
+    const uint32_t v0 = __ldg(D0.cand + r);
+    const uint32_t v1 = __ldg(D1.cand + c1);
+    C.tasks++;
+    C.bytes += 8;
+    if (v0 == v1) return;
+    if (n == 2) {
+        local += 1;
+        return;
+    }
+    uint32_t slot_idx[2] = {0, 0}, slot_vid[2] = {kInvalid, kInvalid};
+    uint32_t pos0 = 0, pos1 = 0, len0 = 0, len1 = 0, vm0 = 0, vm1 = 0;
+    uint64_t ptr0 = 0, ptr1 = 0;
+    if (lane == 0) { slot_idx[0] = r; slot_vid[0] = v0; }
+    if (lane == 1) { slot_idx[0] = c1; slot_vid[0] = v1; }
+    C.nodes += 2;
+    if (n == 3) {
+        local += last_depth_count(P, 2, scr, st, A.gallop_ratio, C, slot_idx, slot_vid);
+        return;
+    }
+    // aliases used by SLOT_GET / SLOT_SET
+#define idx0 slot_idx[0]
+#define idx1 slot_idx[1]
+#define vid0 slot_vid[0]
+#define vid1 slot_vid[1]
+    uint32_t d = 2;
+    auto open_depth = [&](uint32_t dd) {
+        Row r0, r1;
+        const DepthInfo& D = P.dep[dd];
+        const uint32_t k = build_rows<false>(P, D, scr + D.scr_off, st, A.gallop_ratio, C, r0, r1, slot_idx);
+        SLOT_SET(ptr, dd, reinterpret_cast<uint64_t>(r0.p));
+        SLOT_SET(len, dd, k);
+        SLOT_SET(pos, dd, 0u);
+        SLOT_SET(vm, dd, 0u);
+    };
+    open_depth(2);
+    uint32_t iter = 0;
+    for (;;) {
+        if ((++iter & 255u) == 0 && task_should_stop(A, T)) break;
+        uint32_t vm = SLOT_GET(vm, d);
+        if (vm == 0) {
+            const uint32_t pos = SLOT_GET(pos, d);
+            const uint32_t len = SLOT_GET(len, d);
+            if (pos >= len) {
+                if (d == 2) break;
+                --d;
+                continue;
+            }
+            const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+            const DepthInfo& D = P.dep[d];
+            const uint32_t i = pos + lane;
+            uint32_t v = kInvalid;
+            if (i < len) v = __ldg(D.cand + lp[i]);
+            bool clash = false;
+            for (uint32_t j = 0; j < d; ++j) clash |= (SLOT_GET(vid, j) == v);
+            vm = __ballot_sync(kFull, i < len && !clash);
+            C.bytes += 8ull * min(32u, len - pos);
+            SLOT_SET(pos, d, pos + 32);
+            SLOT_SET(vm, d, vm);
+            continue;
+        }
+        const uint32_t b = __ffs(vm) - 1;
+        SLOT_SET(vm, d, vm & (vm - 1));
+        const uint32_t pos = SLOT_GET(pos, d) - 32 + b;
+        const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+        const uint32_t c = lp[pos];
+        const uint32_t v = __ldg(P.dep[d].cand + c);
+        SLOT_SET(idx, d, c);
+        SLOT_SET(vid, d, v);
+        C.nodes++;
+        if (d + 2 == n) {
+            local += last_depth_count(P, n - 1, scr, st, A.gallop_ratio, C, slot_idx, slot_vid);
+            continue;
+        }
+        ++d;
+        open_depth(d);
+    }
+#undef idx0
+#undef idx1
+#undef vid0
+#undef vid1
+}
+
+// ================================================================== cache + failing-set mode
+// explore_Intersection_Cache_DAF_Filter (explore.h:968-1129) with
+// CacheBuffer::getNextCandidatesImpl (explore.h:200-243) and DAFFailingPrune
+// (prune.h:82-171).  Op results are data-vertex lists: ops without a parent
+// alias the adjacency row of the vertex just chosen; the others are
+// parent ∩ N(v) in the op's scratch buffer.  Candidates are filtered by the
+// candidate mask (candidates_exsist, explore.h:998).
+
+struct OpState {  // per warp, in shared memory
+    const uint32_t* p;
+    uint32_t len;
+    uint32_t pad;
+};
+
+// Computes the ops of depth dd for vertex v.  Returns kInvalid on success,
+// else the vdepth of the first empty op (conf_dep).
+__device__ uint32_t compute_ops(const QPlan& P, uint32_t dd, uint32_t v, uint32_t* scr, OpState* ops, Stage& st,
+                                uint32_t gallop_ratio, Counters& C) {
+    const DepthInfo& D = P.dep[dd];
+    const uint64_t o0 = __ldg(P.off + v);
+    const uint32_t dv = (uint32_t)(__ldg(P.off + v + 1) - o0);
+    const uint32_t* nv = P.adj + o0;
+    for (uint32_t k = 0; k < D.nops; ++k) {
+        const uint32_t id = D.ops_begin + k;
+        const OpInfo O = P.op[id];
+        uint32_t len;
+        const uint32_t* p;
+        if (O.parent == kInvalid) {
+            p = nv;
+            len = dv;
+        } else {
+            const OpState par = ops[O.parent];
+            uint32_t* out = scr + O.scr_off;
+            C.isect++;
+            C.bytes += 4ull * (par.len + dv);
+            if (par.len <= dv) len = isect<false>(st, gallop_ratio, par.p, par.len, nv, dv, out);
+            else len = isect<false>(st, gallop_ratio, nv, dv, par.p, par.len, out);
+            p = out;
+        }
+        __syncwarp();
+        if (lane_id() == 0) {
+            ops[id].p = p;
+            ops[id].len = len;
+        }
+        __syncwarp();
+        if (len == 0) return O.vdepth;
+    }
+    return kInvalid;
+}
+
+// Last depth: count list members that are candidates of u_L and not embedded.
+// Returns the count; conf gets the depths of embedded vertices found.
+__device__ uint64_t cache_last_count(const QPlan& P, uint32_t L, const uint32_t* lp, uint32_t len,
+                                     const uint32_t (&slot_vid)[2], uint64_t& conf, Counters& C) {
+    const uint32_t lane = lane_id();
+    const uint32_t u = P.dep[L].u;
+    uint32_t cnt = 0;
+    for (uint32_t base = 0; base < len; base += 32) {
+        const uint32_t i = base + lane;
+        bool ok = false;
+        if (i < len) ok = (__ldg(P.mask + lp[i]) >> u) & 1ull;
+        cnt += __popc(__ballot_sync(kFull, ok));
+    }
+    C.bytes += 12ull * len;
+    // embedded vertices among them: lane j tests the vertex of depth j
+    conf = 0;
+    for (uint32_t half = 0; half < 2; ++half) {
+        const uint32_t j = half * 32 + lane;
+        bool in = false;
+        if (j < L) {
+            const uint32_t v = half ? slot_vid[1] : slot_vid[0];
+            if ((__ldg(P.mask + v) >> u) & 1ull) in = bsearch_global(lp, len, v);
+        }
+        const uint32_t b = __ballot_sync(kFull, in);
+        conf |= (uint64_t)b << (32 * half);
+        if (L <= 32) break;
+    }
+    return (uint64_t)(cnt - __popcll(conf));
+}
+
+__device__ void run_cache_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, OpState* ops, Stage& st,
+                               Counters& C, Tally& T) {
+    unsigned long long& local = T.local;
+    const uint32_t lane = lane_id();
+    const uint32_t n = P.n;
+    const uint64_t ALL = ~0ull;
+    const bool fs = A.failing_sets != 0;
+    C.tasks++;
+    // root (explore.h:1100-1122): v0 = candidates[u0][t]
+    const uint32_t v0 = __ldg(P.dep[0].cand + t);
+    C.bytes += 4;
+    uint32_t slot_vid[2] = {kInvalid, kInvalid};
+    uint32_t pos0 = 0, pos1 = 0, vm0 = 0, vm1 = 0, tot0 = 0, tot1 = 0, skip0 = 0, skip1 = 0;
+    uint64_t fail0 = 0, fail1 = 0, ptr0 = 0, ptr1 = 0;
+    if (lane == 0) slot_vid[0] = v0;
+    C.nodes++;
+#define vid0 slot_vid[0]
+#define vid1 slot_vid[1]
+    // ops of depth 0; an empty op means no extension of this root
+    uint32_t conf = compute_ops(P, 0, v0, scr, ops, st, A.gallop_ratio, C);
+    if (conf != kInvalid) return;
+    auto enter = [&](uint32_t dd) {
+        // candidates of depth dd come from its iteration op (already computed)
+        const OpState it = ops[P.dep[dd].iter_op];
+        SLOT_SET(ptr, dd, reinterpret_cast<uint64_t>(it.p));
+        SLOT_SET(tot, dd, it.len);
+        SLOT_SET(pos, dd, 0u);
+        SLOT_SET(vm, dd, 0u);
+        SLOT_SET(skip, dd, 0u);
+    };
+    auto fail_get = [&](uint32_t dd) -> uint64_t { return shfl64(dd < 32 ? fail0 : fail1, dd & 31); };
+    auto fail_set = [&](uint32_t dd, uint64_t x) { SLOT_SET(fail, dd, x); };
+    // PruneCheck(dd) (prune.h:119-141) with fail[dd] = f just set
+    auto prune_check = [&](uint32_t dd, uint64_t f) {
+        if (!((f >> dd) & 1ull)) {
+            fail_set(dd - 1, f);
+            SLOT_SET(pos, dd, SLOT_GET(tot, dd));
+            SLOT_SET(vm, dd, 0u);
+            C.pruned++;
+        } else {
+            fail_set(dd - 1, fail_get(dd - 1) | f);
+        }
+    };
+    if (fs) fail_set(0, 0ull);
+    uint32_t d = 1;
+    if (n == 2) {
+        uint64_t cf;
+        const OpState it = ops[P.dep[1].iter_op];
+        local += cache_last_count(P, 1, it.p, it.len, slot_vid, cf, C);
+        return;
+    }
+    enter(1);
+    uint32_t iter = 0;
+    for (;;) {
+        if ((++iter & 255u) == 0 && task_should_stop(A, T)) break;
+        uint32_t vm = SLOT_GET(vm, d);
+        if (vm == 0) {
+            const uint32_t pos = SLOT_GET(pos, d);
+            const uint32_t tot = SLOT_GET(tot, d);
+            if (pos >= tot) {
+                // end of depth d: all skipped -> fail[d-1] = anc[d] (explore.h:1068-1070)
+                if (fs && SLOT_GET(skip, d) == tot) fail_set(d - 1, P.dep[d].anc);
+                if (d == 1) break;
+                --d;
+                // PruneCheck(d) after returning from the child (explore.h:1063-1065)
+                if (fs) prune_check(d, fail_get(d));
+                continue;
+            }
+            // next batch: candidates of u_d (mask test); injectivity is checked per pick
+            const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+            const uint32_t u = P.dep[d].u;
+            const uint32_t i = pos + lane;
+            bool isc = false;
+            if (i < tot) isc = (__ldg(P.mask + lp[i]) >> u) & 1ull;
+            const uint32_t cm = __ballot_sync(kFull, isc);
+            const uint32_t nb = min(32u, tot - pos);
+            C.bytes += 12ull * nb;
+            SLOT_SET(skip, d, SLOT_GET(skip, d) + (nb - __popc(cm)));
+            SLOT_SET(pos, d, pos + 32);
+            SLOT_SET(vm, d, cm);
+            continue;
+        }
+        const uint32_t b = __ffs(vm) - 1;
+        SLOT_SET(vm, d, vm & (vm - 1));
+        const uint32_t pos = SLOT_GET(pos, d) - 32 + b;
+        const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+        const uint32_t v = lp[pos];
+        // injectivity with the conflicting depth (explore.h:1014-1022)
+        uint32_t cdep = kInvalid;
+        for (uint32_t half = 0; half < 2; ++half) {
+            const uint32_t bm = __ballot_sync(kFull, (half * 32 + lane) < d && (half ? vid1 : vid0) == v);
+            if (bm && cdep == kInvalid) cdep = half * 32 + __ffs(bm) - 1;
+            if (d <= 32) break;
+        }
+        if (cdep != kInvalid) {
+            if (fs) {
+                const uint64_t f = P.dep[d].anc | P.dep[cdep].anc;
+                fail_set(d, f);
+                fail_set(d - 1, fail_get(d - 1) | f);  // bit d is in anc[d]: never prunes
+            }
+            continue;
+        }
+        SLOT_SET(vid, d, v);
+        C.nodes++;
+        // ops of depth d for v
+        conf = compute_ops(P, d, v, scr, ops, st, A.gallop_ratio, C);
+        if (conf != kInvalid) {
+            // NoCandidatesConflictCheckCache(0, d+1, conf) then PruneCheck(d)
+            if (fs) {
+                const uint64_t f = P.dep[conf].anc;
+                fail_set(d, f);
+                prune_check(d, f);
+            }
+            continue;
+        }
+        if (d + 2 == n) {
+            // child is the last depth: count it in bulk and derive its failing set
+            const OpState it = ops[P.dep[d + 1].iter_op];
+            uint64_t cf = 0;
+            const uint64_t k = cache_last_count(P, d + 1, it.p, it.len, slot_vid, cf, C);
+            local += k;
+            if (fs) {
+                uint64_t f;
+                if (k > 0) {
+                    f = ALL;  // SuccessMatch (prune.h:143-146)
+                } else {
+                    f = P.dep[d + 1].anc;  // all skipped, or conflicts: anc[L] | anc[conflict depths]
+                    uint64_t m = cf;
+                    while (m) {
+                        const int j = __ffsll((long long)m) - 1;
+                        m &= m - 1;
+                        f |= P.dep[j].anc;
+                    }
+                }
+                fail_set(d, f);
+                prune_check(d, f);
+            }
+            continue;
+        }
+        // descend: the child's entry resets its parent's accumulator (prune.h:162)
+        ++d;
+        if (fs) fail_set(d - 1, 0ull);
+        enter(d);
+    }
+#undef vid0
+#undef vid1
+}
+
+// ================================================================== kernel
+__global__ void __launch_bounds__(256) enum_kernel(EnumArgs A) {
+    SMX_EXTERN_SMEM(smem);
+    const uint32_t lane = lane_id();
+    const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    // shared layout: [wpb][stage buffer] [wpb][mbarrier] [wpb][max_ops op states]
+    const size_t stage_bytes = ((size_t)(A.chunk + 8) * 4 + 15) & ~(size_t)15;
+    Stage st;
+    st.buf = reinterpret_cast<uint32_t*>(smem + stage_bytes * wib);
+    st.mbar = reinterpret_cast<uint64_t*>(smem + stage_bytes * wpb) + wib;
+    st.phase = 0;
+    st.chunk = A.chunk;
+    st.tma = A.use_tma != 0;
+    st.failed = false;
+    OpState* wops = reinterpret_cast<OpState*>(smem + stage_bytes * wpb + 16 * wpb) + (size_t)wib * A.max_ops;
+#ifndef SMX_EMU
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(st.mbar)) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+#else
+    st.tma = false;
+#endif
+    __syncwarp();
+    uint32_t* scr = A.scratch + (size_t)gw * A.scratch_stride;
+    const uint64_t deadline = A.budget_ns ? global_timer_ns() + A.budget_ns : 0;
+    Counters C;
+    Tally T;
+    const uint64_t total = A.task_prefix[A.nq];
+    uint32_t q = 0;
+    uint64_t qlo = A.task_prefix[0], qhi = A.task_prefix[1];
+    uint32_t grabs = 0;
+    for (;;) {
+        unsigned long long t0 = 0;
+        if (lane == 0) t0 = atomicAdd(A.next_task, (unsigned long long)A.grab);
+        t0 = __shfl_sync(kFull, t0, 0);
+        if (t0 >= total) break;
+        if ((grabs++ & 63u) == 0) check_global_stop(A, deadline);
+        if (poll_abort(A)) break;
+        const uint64_t t1 = min((uint64_t)t0 + A.grab, total);
+        for (uint64_t t = t0; t < t1; ++t) {
+            if (t < qlo || t >= qhi) {
+                uint32_t lo = 0, hi = A.nq;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (A.task_prefix[mid] <= t) lo = mid; else hi = mid;
+                }
+                q = lo;
+                qlo = A.task_prefix[q];
+                qhi = A.task_prefix[q + 1];
+            }
+            if (query_stopped(A, q)) continue;
+            const QPlan& P = A.plans[q];
+            T.q = q;
+            T.local = 0;
+            if (P.mode == SMX_EXPLORE_CANDIDATES) run_table_task(A, P, t - qlo, scr, st, C, T);
+            else run_cache_task(A, P, t - qlo, scr, wops, st, C, T);
+            flush_tally(A, T);
+            if (st.failed) break;
+        }
+        if (st.failed) {
+            if (lane == 0) atomicCAS(A.status, 0, (int)SMX_CUDA_ERROR);
+            break;
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(A.stats + 0, C.isect);
+        atomicAdd(A.stats + 1, C.nodes);
+        atomicAdd(A.stats + 2, C.bytes);
+        atomicAdd(A.stats + 3, C.tasks);
+        atomicAdd(A.stats + 4, C.pruned);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+struct HostPlanBuild {
+    QPlan plan;
+    std::vector<BnRef> bn;
+    std::vector<OpInfo> op;
+    uint64_t scratch_elems = 0;
+};
+
+int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order, int mode,
+                    HostPlanBuild& hb) {
+    const uint32_t n = q.n;
+    std::memset(&hb.plan, 0, sizeof(QPlan));
+    QPlan& P = hb.plan;
+    P.n = n;
+    P.qn = c->qn;
+    P.mode = (uint32_t)mode;
+    P.rank = c->d_rank;
+    P.mask = c->d_mask;
+    P.off = g->d_off;
+    P.adj = g->d_adj;
+    P.nroot = c->cnt[order[0]];
+    std::vector<uint32_t> depth_of(n);
+    for (uint32_t i = 0; i < n; ++i) depth_of[order[i]] = i;
+    // backward neighbours ordered by position (GetPreviousNeb, common_ops.h:259-306)
+    std::vector<std::vector<uint32_t>> bnd(n);
+    for (uint32_t dd = 0; dd < n; ++dd) {
+        const uint32_t u = order[dd];
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            const uint32_t p = depth_of[q.adj[e]];
+            if (p < dd) bnd[dd].push_back(p);
+        }
+        std::sort(bnd[dd].begin(), bnd[dd].end());
+        if (dd > 0 && bnd[dd].empty()) return fail(SMX_INVALID_ORDER, "order has a vertex without an earlier neighbour");
+    }
+    // DAF ancestors (prune.h:100-104)
+    std::vector<uint64_t> anc(n, 0);
+    for (uint32_t dd = 0; dd < n; ++dd) {
+        anc[dd] = 1ull << dd;
+        for (uint32_t p : bnd[dd]) anc[dd] |= anc[p];
+    }
+    uint64_t scr = 0;
+    for (uint32_t dd = 0; dd < n; ++dd) {
+        DepthInfo& D = P.dep[dd];
+        D.u = order[dd];
+        D.cand = c->cand_ptr(order[dd]);
+        D.nbn = (uint32_t)bnd[dd].size();
+        D.bn_begin = (uint32_t)hb.bn.size();
+        D.anc = anc[dd];
+        D.iter_op = kInvalid;
+        uint32_t cap = 0xffffffffu;
+        for (uint32_t p : bnd[dd]) {
+            BnRef r{};
+            r.depth = p;
+            if (mode == SMX_EXPLORE_CANDIDATES) {
+                const int ti = c->tab_index[order[p]][order[dd]];
+                if (ti < 0)
+                    return fail(SMX_BAD_ARGUMENT,
+                                "candidate-table enumeration needs the edge tables (smx_filter build_tables=1)");
+                const DevTable& T = c->tables[ti];
+                r.off = T.d_off;
+                r.edge = T.d_edge;
+                r.max_deg = T.max_deg;
+                cap = std::min(cap, T.max_deg);
+            }
+            hb.bn.push_back(r);
+        }
+        D.scr_off = 0;
+        if (mode == SMX_EXPLORE_CANDIDATES && dd >= 2 && D.nbn >= 2) {
+            D.scr_off = (uint32_t)scr;
+            // result <= min row <= cap; a second cap for the >32-neighbour swap
+            const uint64_t need = (uint64_t)cap * (D.nbn > 32 ? 2 : 1);
+            scr += (need + 8 + 3) & ~3ull;  // 16-byte aligned buffers
+        }
+    }
+    if (mode == SMX_EXPLORE_CANDIDATES) {
+        P.ntasks = n >= 2 ? c->tables[c->tab_index[order[0]][order[1]]].e_cnt : 0;
+    } else {
+        Plan plan;
+        if (!build_plan(q, order, plan)) return fail(SMX_INVALID_ORDER, "order has a vertex without an earlier neighbour");
+        P.nops = (uint32_t)plan.ops.size();
+        // op ids renumbered so the ops of each depth are contiguous
+        std::vector<uint32_t> newid(plan.ops.size(), kInvalid);
+        uint32_t next = 0;
+        for (uint32_t dd = 0; dd < n; ++dd)
+            for (uint32_t id : plan.ops_at[dd]) newid[id] = next++;
+        hb.op.assign(plan.ops.size(), OpInfo{});
+        for (uint32_t id = 0; id < plan.ops.size(); ++id) {
+            const PlanOp& po = plan.ops[id];
+            OpInfo& oi = hb.op[newid[id]];
+            oi.parent = po.parent == kInvalid ? kInvalid : newid[po.parent];
+            oi.vdepth = po.vdepth;
+            oi.scr_off = 0;
+            if (po.parent != kInvalid) {
+                oi.scr_off = (uint32_t)scr;
+                scr += ((uint64_t)g->h.max_deg + 8 + 3) & ~3ull;
+            }
+        }
+        next = 0;
+        for (uint32_t dd = 0; dd < n; ++dd) {
+            P.dep[dd].ops_begin = next;
+            P.dep[dd].nops = (uint32_t)plan.ops_at[dd].size();
+            next += P.dep[dd].nops;
+            P.dep[dd].iter_op = dd ? newid[plan.iter_op[dd]] : kInvalid;
+        }
+        P.ntasks = c->cnt[order[0]];
+    }
+    hb.scratch_elems = scr + 8;
+    return SMX_OK;
+}
+
+}  // namespace
+
+int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, const std::vector<const smx_cand*>& cs,
+                     const std::vector<const uint32_t*>& orders, const smx_enum_opts& o,
+                     const std::vector<uint64_t>& limits, volatile uint32_t* stop, uint64_t* counts, smx_stats* st,
+                     bool use_graph) {
+    SMX_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const uint32_t nq = (uint32_t)qs.size();
+    if (nq == 0) return SMX_OK;
+    const int mode = o.explore;
+    std::vector<HostPlanBuild> hb(nq);
+    std::vector<uint64_t> prefix(nq + 1, 0);
+    uint64_t scratch_elems = 8;
+    uint32_t max_ops = 1;
+    for (uint32_t i = 0; i < nq; ++i) {
+        int rc = build_host_plan(g, *qs[i], cs[i], orders[i], mode, hb[i]);
+        if (rc != SMX_OK) return rc;
+        scratch_elems = std::max(scratch_elems, hb[i].scratch_elems);
+        max_ops = std::max(max_ops, hb[i].plan.nops);
+        prefix[i + 1] = prefix[i] + hb[i].plan.ntasks;
+    }
+    // device copies of plans; bn / op arrays in one pool
+    size_t pool_bytes = 64;
+    for (auto& h : hb) pool_bytes += h.bn.size() * sizeof(BnRef) + h.op.size() * sizeof(OpInfo) + 32;
+    std::vector<char> pool(pool_bytes, 0);
+    std::vector<QPlan> plans(nq);
+    char* d_pool = nullptr;
+    QPlan* d_plans = nullptr;
+    SMX_CUDA_TRY(cudaMallocAsync(&d_pool, pool_bytes, s));
+    SMX_CUDA_TRY(cudaMallocAsync(&d_plans, nq * sizeof(QPlan), s));
+    size_t at = 0;
+    for (uint32_t i = 0; i < nq; ++i) {
+        plans[i] = hb[i].plan;
+        at = (at + 15) & ~(size_t)15;
+        if (!hb[i].bn.empty()) std::memcpy(pool.data() + at, hb[i].bn.data(), hb[i].bn.size() * sizeof(BnRef));
+        plans[i].bn = reinterpret_cast<const BnRef*>(d_pool + at);
+        at += hb[i].bn.size() * sizeof(BnRef);
+        at = (at + 15) & ~(size_t)15;
+        if (!hb[i].op.empty()) std::memcpy(pool.data() + at, hb[i].op.data(), hb[i].op.size() * sizeof(OpInfo));
+        plans[i].op = reinterpret_cast<const OpInfo*>(d_pool + at);
+        at += hb[i].op.size() * sizeof(OpInfo);
+    }
+    SMX_CUDA_TRY(cudaMemcpyAsync(d_pool, pool.data(), pool_bytes, cudaMemcpyHostToDevice, s));
+    SMX_CUDA_TRY(cudaMemcpyAsync(d_plans, plans.data(), nq * sizeof(QPlan), cudaMemcpyHostToDevice, s));
+    // launch shape
+    const uint32_t wpb = o.warps_per_block > 0 ? std::min<uint32_t>((uint32_t)o.warps_per_block, 8u) : 8u;
+    const uint32_t chunk = o.stage_chunk > 0 ? ((uint32_t)o.stage_chunk + 3) & ~3u : 1024u;
+    const size_t stage_bytes = ((size_t)(chunk + 8) * 4 + 15) & ~(size_t)15;
+    const size_t smem = stage_bytes * wpb + 16 * wpb + (size_t)max_ops * sizeof(OpState) * wpb;
+    if (smem > 227 * 1024)
+        return fail(SMX_TOO_LARGE, "shared memory per block above 227 KB: lower stage_chunk or warps_per_block");
+    SMX_CUDA_TRY(cudaFuncSetAttribute(enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int bps = 0;
+    SMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, enum_kernel, (int)(wpb * 32), smem));
+    if (o.blocks_per_sm > 0) bps = std::min(bps, o.blocks_per_sm);
+    if (bps < 1) return fail(SMX_TOO_LARGE, "enumeration kernel does not fit on an SM with this shared-memory size");
+    const uint32_t blocks = (uint32_t)(g->num_sms * bps);
+    const uint64_t nwarps = (uint64_t)blocks * wpb;
+    // control block (explicit offsets) + per-warp scratch
+    const size_t o_next = 0, o_status = 8, o_stats = 16;           // stats: 5 x u64
+    const size_t o_qcount = 64;
+    const size_t o_qlimit = o_qcount + (size_t)nq * 8;
+    const size_t o_prefix = o_qlimit + (size_t)nq * 8;
+    const size_t o_qstop = o_prefix + (size_t)(nq + 1) * 8;
+    const size_t o_scr = (o_qstop + (size_t)nq * 4 + 255) & ~(size_t)255;
+    const size_t total_bytes = o_scr + nwarps * scratch_elems * 4 + 64;
+    int rc = ensure_scratch(g, total_bytes);
+    if (rc != SMX_OK) return rc;
+    char* base = static_cast<char*>(g->d_scratch);
+    unsigned long long* d_next = reinterpret_cast<unsigned long long*>(base + o_next);
+    int* d_status = reinterpret_cast<int*>(base + o_status);
+    unsigned long long* d_stats = reinterpret_cast<unsigned long long*>(base + o_stats);
+    unsigned long long* d_qcount = reinterpret_cast<unsigned long long*>(base + o_qcount);
+    uint64_t* d_qlimit = reinterpret_cast<uint64_t*>(base + o_qlimit);
+    uint64_t* d_prefix = reinterpret_cast<uint64_t*>(base + o_prefix);
+    uint32_t* d_qstop = reinterpret_cast<uint32_t*>(base + o_qstop);
+    uint32_t* d_scr = reinterpret_cast<uint32_t*>(base + o_scr);
+    SMX_CUDA_TRY(cudaMemcpyAsync(d_qlimit, limits.data(), nq * 8, cudaMemcpyHostToDevice, s));
+    SMX_CUDA_TRY(cudaMemcpyAsync(d_prefix, prefix.data(), (nq + 1) * 8, cudaMemcpyHostToDevice, s));
+    // host-visible stop word: the device polls a mapped pointer
+    const volatile uint32_t* d_host_stop = nullptr;
+    if (stop) {
+        void* dp = nullptr;
+        if (cudaHostGetDevicePointer(&dp, (void*)stop, 0) == cudaSuccess) d_host_stop = static_cast<const volatile uint32_t*>(dp);
+        else cudaGetLastError();
+    }
+    EnumArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.plans = d_plans;
+    A.task_prefix = d_prefix;
+    A.next_task = d_next;
+    A.qcount = d_qcount;
+    A.qstop = d_qstop;
+    A.qlimit = d_qlimit;
+    A.scratch = d_scr;
+    A.stats = d_stats;
+    A.status = d_status;
+    A.host_stop = d_host_stop;
+    A.scratch_stride = scratch_elems;
+    A.budget_ns = o.time_budget_ms > 0 ? (uint64_t)(o.time_budget_ms * 1e6) : 0;
+    A.nq = nq;
+    A.max_ops = max_ops;
+    A.grab = o.task_grab > 0 ? (uint32_t)o.task_grab : 4u;
+    A.chunk = chunk;
+    A.gallop_ratio = o.gallop_ratio > 0 ? (uint32_t)o.gallop_ratio : 16u;
+    A.use_tma = o.use_tma ? 1u : 0u;
+    A.failing_sets = o.failing_sets ? 1u : 0u;
+    cudaEvent_t e0, e1;
+    SMX_CUDA_TRY(cudaEventCreate(&e0));
+    SMX_CUDA_TRY(cudaEventCreate(&e1));
+    auto record = [&](cudaStream_t ss) -> cudaError_t {
+        cudaError_t e;
+        if ((e = cudaMemsetAsync(base, 0, 64, ss)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(d_qcount, 0, nq * 8, ss)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(d_qstop, 0, nq * 4, ss)) != cudaSuccess) return e;
+        SMX_LAUNCH(enum_kernel, blocks, wpb * 32, smem, ss, A);
+        return cudaGetLastError();
+    };
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (use_graph) {
+        SMX_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t ce = record(s);
+        cudaError_t ee = cudaStreamEndCapture(s, &graph);
+        if (ce != cudaSuccess) return fail(SMX_CUDA_ERROR, std::string("capture: ") + cudaGetErrorString(ce));
+        if (ee != cudaSuccess) return fail(SMX_CUDA_ERROR, std::string("end capture: ") + cudaGetErrorString(ee));
+        SMX_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+        SMX_CUDA_TRY(cudaEventRecord(e0, s));
+        SMX_CUDA_TRY(cudaGraphLaunch(exec, s));
+        SMX_CUDA_TRY(cudaEventRecord(e1, s));
+    } else {
+        SMX_CUDA_TRY(cudaEventRecord(e0, s));
+        cudaError_t ce = record(s);
+        if (ce != cudaSuccess) return fail(SMX_CUDA_ERROR, std::string("enumeration launch: ") + cudaGetErrorString(ce));
+        SMX_CUDA_TRY(cudaEventRecord(e1, s));
+    }
+    SMX_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    SMX_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::vector<unsigned long long> qc(nq);
+    unsigned long long stats[5];
+    int status = 0;
+    SMX_CUDA_TRY(cudaMemcpy(qc.data(), d_qcount, nq * 8, cudaMemcpyDeviceToHost));
+    SMX_CUDA_TRY(cudaMemcpy(stats, d_stats, sizeof(stats), cudaMemcpyDeviceToHost));
+    SMX_CUDA_TRY(cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    SMX_CUDA_TRY(cudaFreeAsync(d_pool, s));
+    SMX_CUDA_TRY(cudaFreeAsync(d_plans, s));
+    SMX_CUDA_TRY(cudaStreamSynchronize(s));
+    uint64_t raw = 0, capped = 0;
+    bool reached = false;
+    for (uint32_t i = 0; i < nq; ++i) {
+        raw += qc[i];
+        uint64_t c = qc[i];
+        if (limits[i] && c >= limits[i]) {
+            c = limits[i];
+            reached = true;
+        }
+        capped += c;
+        if (counts) counts[i] = c;
+    }
+    if (st) {
+        st->count = capped;
+        st->raw_count = raw;
+        st->intersections = stats[0];
+        st->nodes = stats[1];
+        st->bytes = stats[2];
+        st->tasks = stats[3];
+        st->pruned = stats[4];
+        st->kernel_ms = ms;
+        st->limit_reached = reached ? 1 : 0;
+        st->status = status;
+    }
+    if (status == SMX_CUDA_ERROR) return fail(SMX_CUDA_ERROR, "bulk copy wait did not complete; enumeration aborted");
+    if (status == SMX_TIMEOUT) set_error("time budget exhausted; the count is partial");
+    if (status == SMX_STOPPED) set_error("stopped by the caller; the count is partial");
+    return status;
+}
+
+int ensure_scratch(smx_graph* g, size_t bytes) {
+    if (g->scratch_bytes >= bytes) return SMX_OK;
+    if (g->d_scratch) SMX_CUDA_TRY(cudaFree(g->d_scratch));
+    g->d_scratch = nullptr;
+    g->scratch_bytes = 0;
+    SMX_CUDA_TRY(cudaMalloc(&g->d_scratch, bytes));
+    g->scratch_bytes = bytes;
+    return SMX_OK;
+}
+
+}  // namespace smx

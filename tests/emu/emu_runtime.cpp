@@ -1,0 +1,133 @@
+// Runtime half of the CPU stand-in (see cuda_runtime.h).  TEST INFRASTRUCTURE ONLY.
+#include "cuda_runtime.h"
+
+namespace emu {
+thread_local Ctx ctx;
+
+Capture& capture() {
+    static thread_local Capture c;
+    return c;
+}
+
+uint64_t timer_ns() {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+}  // namespace emu
+
+struct EmuEvent {
+    uint64_t t = 0;
+};
+struct EmuGraph {
+    std::vector<std::function<void()>> ops;
+};
+
+cudaError_t cudaGetDeviceCount(int* n) {
+    *n = 1;
+    return cudaSuccess;
+}
+cudaError_t cudaSetDevice(int) { return cudaSuccess; }
+cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr, int) {
+    *v = 1;  // one "SM": launches shrink to a handful of blocks
+    return cudaSuccess;
+}
+cudaError_t cudaStreamCreateWithFlags(cudaStream_t* s, unsigned) {
+    *s = reinterpret_cast<cudaStream_t>(0x1);
+    return cudaSuccess;
+}
+cudaError_t cudaStreamDestroy(cudaStream_t) { return cudaSuccess; }
+cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+static void* poisoned_alloc(size_t n) {
+    const size_t sz = ((n ? n : 1) + 255) & ~(size_t)255;
+    void* p = std::aligned_alloc(256, sz);
+    if (p) std::memset(p, 0xCD, sz);  // poison: no zeroed memory may be assumed
+    return p;
+}
+cudaError_t cudaMalloc(void** p, size_t n) {
+    *p = poisoned_alloc(n);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaMallocAsync(void** p, size_t n, cudaStream_t) {
+    *p = poisoned_alloc(n);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFree(void* p) {
+    std::free(p);
+    return cudaSuccess;
+}
+cudaError_t cudaFreeAsync(void* p, cudaStream_t) {
+    std::free(p);
+    return cudaSuccess;
+}
+cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
+    std::memmove(d, s, n);
+    return cudaSuccess;
+}
+cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind, cudaStream_t) {
+    std::memmove(d, s, n);
+    return cudaSuccess;
+}
+cudaError_t cudaMemset(void* p, int v, size_t n) {
+    std::memset(p, v, n);
+    return cudaSuccess;
+}
+cudaError_t cudaMemsetAsync(void* p, int v, size_t n, cudaStream_t) {
+    if (emu::capture().on) {
+        emu::capture().ops.push_back([=]() { std::memset(p, v, n); });
+        return cudaSuccess;
+    }
+    std::memset(p, v, n);
+    return cudaSuccess;
+}
+cudaError_t cudaEventCreate(cudaEvent_t* e) {
+    *e = new EmuEvent();
+    return cudaSuccess;
+}
+cudaError_t cudaEventDestroy(cudaEvent_t e) {
+    delete e;
+    return cudaSuccess;
+}
+cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t) {
+    e->t = emu::timer_ns();
+    return cudaSuccess;
+}
+cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
+cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t a, cudaEvent_t b) {
+    *ms = (float)((double)(b->t - a->t) / 1e6);
+    return cudaSuccess;
+}
+cudaError_t cudaGetLastError() { return cudaSuccess; }
+const char* cudaGetErrorString(cudaError_t e) { return e == cudaSuccess ? "no error" : "emulated error"; }
+cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned) {
+    *d = h;
+    return cudaSuccess;
+}
+cudaError_t cudaStreamBeginCapture(cudaStream_t, cudaStreamCaptureMode) {
+    emu::capture().on = true;
+    emu::capture().ops.clear();
+    return cudaSuccess;
+}
+cudaError_t cudaStreamEndCapture(cudaStream_t, cudaGraph_t* g) {
+    auto* gr = new EmuGraph();
+    gr->ops.swap(emu::capture().ops);
+    emu::capture().on = false;
+    *g = gr;
+    return cudaSuccess;
+}
+cudaError_t cudaGraphInstantiate(cudaGraphExec_t* e, cudaGraph_t g, unsigned long long) {
+    *e = new EmuGraph(*g);
+    return cudaSuccess;
+}
+cudaError_t cudaGraphLaunch(cudaGraphExec_t e, cudaStream_t) {
+    for (auto& op : e->ops) op();
+    return cudaSuccess;
+}
+cudaError_t cudaGraphExecDestroy(cudaGraphExec_t e) {
+    delete e;
+    return cudaSuccess;
+}
+cudaError_t cudaGraphDestroy(cudaGraph_t g) {
+    delete g;
+    return cudaSuccess;
+}
