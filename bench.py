@@ -1,0 +1,397 @@
+"""Benchmark of the filter -> edge table -> enumerate path on B200.
+
+Workload (the plain method at scale): a seeded Chung-Lu data graph with
+1,000,000 vertices and 10,000,000 edges (degree exponent 2.2, unlabelled,
+int32 neighbour ids), 100 seeded queries of 8 and 12 vertices (half dense:
+greedy-densest growth, average degree > 3; half sparse: random-walk edges),
+GQL filter, RI order, exhaustive counts capped at 10^9 per query.  Synthetic
+data stands in for datasets (no network).
+
+One step = the whole pipeline for one batch of 10 queries: NLF + GQL
+filtering, candidate-edge tables, enumeration.  Steps walk through the
+100-query workload batch by batch (warm-up on the first batches, timed steps
+on the next ones).  `value` is queries/s over all
+ranks with the data graph resident in HBM; `e2e` runs the same through the C
+ABI from pinned host buffers (data-graph CSR upload, queries, counts back)
+inside the timed region.  L2 (126 MB) is flushed before every timed step.
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own 100
+queries on a replica of the data graph (weak scaling, no data-path
+collective); rank 0 prints the line with times = max over ranks.
+
+--impl reference runs the reference's own CPU code (oracle/_ref, built from
+the reference sources) on a bounded sample per step: the GQL filter of one
+query and its enumeration to a reduced cap with all host threads, scaled to
+queries/s by the measured embedding rate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_VERT = 1_000_000
+N_EDGE = 10_000_000
+GAMMA = 2.2
+GRAPH_SEED = 2
+CAP = 1_000_000_000
+WORKLOAD = "cfg2: Chung-Lu 1M V / 10M E (gamma 2.2), 100 queries of 8/12 vertices (half dense), GQL + RI, cap 1e9"
+METRIC = "queries/s & embeddings/s; learned-order vs RI-order GPU speedup at exact counts"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=10, help="queries per step")
+    ap.add_argument("--impl", default="smx", choices=["smx", "reference"])
+    ap.add_argument("--queries", type=int, default=100)
+    ap.add_argument("--cap", type=int, default=CAP)
+    ap.add_argument("--explore", type=int, default=0, help="0 candidate tables, 1 cache + failing sets")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def query_specs(nq: int, rank: int):
+    """(k, dense, seed) per query: sizes 8 / 12, dense and sparse alternating."""
+    out = []
+    for i in range(nq):
+        k = 8 if (i // 2) % 2 == 0 else 12
+        out.append((k, i % 2 == 0, 10_000 + rank * 100_000 + i))
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="smx_clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM traffic of the enumeration kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "enum_kernel_cfg2.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "smx" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        import datetime
+
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if pg.get_backend() == "nccl" else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ---------------------------------------------------------------------- reference arm
+def run_reference(args, world, rank, pg):
+    if rank != 0:
+        return
+    from oracle import GQL, RefOracle, available
+
+    if not available()["ref"]:
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle library not built (oracle/_ref)"}))
+        return
+    line = reference_sample(args, steps=args.steps, warmup=args.warmup)
+    line["impl"] = "reference"
+    line["e2e"] = {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
+
+
+def reference_sample(args, steps: int, warmup: int, sample_cap: int = 20_000_000):
+    """The reference (oracle/_ref) on a bounded sample: per step one query's
+    GQL filter + RI order + enumeration to sample_cap with all host threads;
+    queries/s is scaled from the filter time and the embedding rate to the
+    workload's cap."""
+    import subgraphmatching_b200 as smx
+    from oracle import GQL, RefOracle
+
+    R = RefOracle()
+    threads = os.cpu_count() or 1
+    g = smx.Graph.generate(N_VERT, N_EDGE, GAMMA, 1, 1.0, GRAPH_SEED, device=-1)
+    tmp = tempfile.mkdtemp(prefix="smx_ref_")
+    gpath = os.path.join(tmp, "data.txt")
+    g.save(gpath)
+    gr = R.load_graph(gpath)
+    specs = query_specs(args.queries, 0)
+    per_query_s = []
+    emb_rates = []
+    for step in range(warmup + steps):
+        k, dense, seed = specs[step % len(specs)]
+        q = smx.Query.generate(g, k, dense, seed)
+        qpath = os.path.join(tmp, f"q{step}.txt")
+        q.save(qpath)
+        qr = R.load_query(qpath)
+        t0 = time.perf_counter()
+        c = R.filter(gr, qr, GQL)
+        t_filter = time.perf_counter() - t0
+        order = R.order_ri(qr)
+        t0 = time.perf_counter()
+        cnt, _, _ = R.explore(gr, qr, c, order, sample_cap, threads, R.CANDIDATES)
+        t_enum = time.perf_counter() - t0
+        rate = cnt / t_enum if t_enum > 0 else 0.0
+        # a capped count reaches the workload cap at the measured rate; an exhaustive one is done
+        t_full = t_filter + (args.cap / rate if cnt >= sample_cap and rate > 0 else t_enum)
+        if step >= warmup:
+            per_query_s.append(t_full)
+            emb_rates.append(rate)
+    mean_s = sum(per_query_s) / len(per_query_s)
+    return {
+        "metric": METRIC,
+        "value": 1.0 / mean_s,
+        "unit": "queries/s",
+        "n_gpus": 0,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": mean_s * 1000.0,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded Chung-Lu graph and queries)",
+        "config": {"workload": WORKLOAD, "cap": args.cap, "sample_cap": sample_cap},
+        "embeddings_per_s": statistics.mean(emb_rates),
+        "cpu_baseline": {"value": 1.0 / mean_s, "unit": "queries/s", "cores": threads, "kind": "reference",
+                         "sample": f"{steps} queries of the workload (after {warmup} warm-up), each: reference "
+                                   f"Filter_GQL (1 thread) + Order_RI + explore_Intersection_Recursive to "
+                                   f"{sample_cap:,} embeddings on {threads} threads, scaled to the {args.cap:,} cap "
+                                   f"by the measured embedding rate"},
+    }
+
+
+# ---------------------------------------------------------------------- smx arm
+def run_smx(args, world, rank, local, pg):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import subgraphmatching_b200 as smx
+    from subgraphmatching_b200 import _lib
+
+    torch.cuda.set_device(local)
+    dev = local
+    hg = smx.Graph.generate(N_VERT, N_EDGE, GAMMA, 1, 1.0, GRAPH_SEED, device=-1)
+    off, nb, lab = hg.csr()
+    dg = smx.Graph.from_csr(off, nb, lab, device=dev)
+    specs = query_specs(args.queries, rank)
+    queries = [smx.Query.generate(hg, k, dense, seed) for k, dense, seed in specs]
+    nb_batches = max(1, (len(queries) + args.batch - 1) // args.batch)
+    batches = [queries[i * args.batch:(i + 1) * args.batch] for i in range(nb_batches)]
+    opts = smx.EnumOptions(explore=args.explore)
+    build_tables = args.explore == 0
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def step(graph, batch):
+        embeddings = 0
+        kernel_ms = 0.0
+        kbytes = 0
+        for q in batch:
+            can = smx.CandidateParam(graph, q, build_tables=build_tables)
+            if smx.Filter_GQL(graph, q, can):
+                st = smx.explore(graph, q, can, None, opts, args.cap)
+                embeddings += st.count
+                kernel_ms += st.kernel_ms
+                kbytes += st.bytes
+        return embeddings, kernel_ms, kbytes
+
+    for i in range(args.warmup):
+        step(dg, batches[i % nb_batches])
+    first = args.warmup  # timed steps continue through the workload
+    # ---- timed: device-resident inputs
+    times, emb, kms, kby = [], 0, 0.0, 0
+    launches0 = _lib.lib.smx_launch_count()
+    clocks = Clocks(dev)
+    clocks.start()
+    nq_timed = 0
+    for i in range(args.steps):
+        batch = batches[(first + i) % nb_batches]
+        nq_timed += len(batch)
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(pg)
+        _lib.check(_lib.lib.smx_mark_begin(dg._h))
+        e, km, kb = step(dg, batch)
+        ms = ctypes.c_double()
+        _lib.check(_lib.lib.smx_mark_end(dg._h, ctypes.byref(ms)))
+        torch.cuda.synchronize()
+        barrier(pg)
+        times.append(ms.value)
+        emb += e
+        kms += km
+        kby += kb
+    clock_info = clocks.stop()
+    launches = _lib.lib.smx_launch_count() - launches0
+    step_ms = max_over_ranks(pg, sum(times) / len(times))
+    # ---- e2e: pinned host CSR -> device graph, queries, counts back, per step
+    p_off = torch.from_numpy(off.view(np.int64)).pin_memory()
+    p_nb = torch.from_numpy(nb.view(np.int32)).pin_memory()
+    p_lab = torch.from_numpy(lab.view(np.int32)).pin_memory()
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    e2e_times = []
+    for i in range(max(1, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(pg)
+        t0 = time.perf_counter()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib.smx_graph_create(ctypes.cast(p_off.data_ptr(), u64p), ctypes.cast(p_nb.data_ptr(), u32p),
+                                             ctypes.cast(p_lab.data_ptr(), u32p), N_VERT, int(off[-1]), dev,
+                                             ctypes.byref(h)))
+        g2 = smx.Graph(h)
+        step(g2, batches[(first + i) % nb_batches])
+        del g2
+        torch.cuda.synchronize()
+        e2e_times.append((time.perf_counter() - t0) * 1000.0)
+        barrier(pg)
+    e2e_ms = max_over_ranks(pg, sum(e2e_times) / len(e2e_times))
+    b0 = batches[first % nb_batches]
+    h2d = off.nbytes + nb.nbytes + lab.nbytes + sum(q.csr()[0].nbytes + q.csr()[1].nbytes + q.csr()[2].nbytes
+                                                    for q in b0)
+    d2h = 8 * len(b0) * 3  # counts + stats read back per query
+    if rank != 0:
+        return
+    q_per_step = nq_timed / args.steps * world
+    value = q_per_step / (step_ms / 1000.0)
+    hbm, peak_kind = peaks()
+    achieved = (kby / 1e9) / (kms / 1000.0) if kms > 0 else 0.0
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded Chung-Lu graph and queries; no dataset download)",
+        "config": {"workload": WORKLOAD, "queries_per_gpu": len(queries), "queries_per_step": args.batch,
+                   "cap": args.cap,
+                   "explore": "candidate tables" if args.explore == 0 else "cache + failing sets",
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "embeddings_per_s": emb * world / (sum(times) / 1000.0),
+        "e2e": {"value": q_per_step / (e2e_ms / 1000.0), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if hbm else None, "traffic": ncu_traffic(),
+                     "kernel": "enum_kernel", "peak_kind": peak_kind,
+                     "note": "achieved = algorithmic bytes (list elements touched x 4 + row/candidate reads) / "
+                             "event-timed kernel time, summed over the timed launches"},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            ref = reference_sample(args, steps=1, warmup=0)
+            line["cpu_baseline"] = ref["cpu_baseline"]
+        except Exception as e:  # the reference build may be absent
+            line["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, pg)
+        else:
+            run_smx(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

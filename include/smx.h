@@ -92,6 +92,13 @@ const char* smx_status_str(int status);
 const char* smx_last_error(void); /* thread-local message of the last failing call */
 int smx_device_count(void);
 
+/* Device-time markers on the graph's stream (CUDA events): begin records,
+ * end records, waits and returns the elapsed device time in ms. */
+int smx_mark_begin(smx_graph* g);
+int smx_mark_end(smx_graph* g, double* ms);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t smx_launch_count(void);
+
 /* ------------------------------------------------------------ data graph */
 /* Graph from a host CSR (rows strictly ascending, no self loops).
  * Replaces Graph::Load's in-memory result (graph.h:190-266). labels may be NULL (all 0).
@@ -117,9 +124,10 @@ int smx_query_create(const uint32_t* offsets, const uint32_t* neighbors, const u
                      uint32_t num_vertices, smx_query** out);
 /* Query::Load (graph.h:474-478). */
 int smx_query_load_text(const char* path, smx_query** out);
-/* Seeded random-walk query of num_vertices vertices from the data graph, labels inherited.
- * dense != 0: induced subgraph on the walk's vertices (retries until average degree > 3,
- * else the densest seen); dense == 0: only the edges the walk traversed. */
+/* Seeded query of num_vertices vertices taken from the data graph, labels inherited.
+ * dense == 0: a random walk's vertices with only the edges the walk traversed;
+ * dense != 0: a randomized greedy-densest growth from a seeded start, induced subgraph
+ * (retried until the average degree exceeds 3, else the densest attempt). */
 int smx_query_generate(const smx_graph* g, uint32_t num_vertices, int dense, uint64_t seed, smx_query** out);
 int smx_query_info(const smx_query* q, uint32_t* num_vertices, uint32_t* num_edges, uint32_t* max_degree);
 int smx_query_export(const smx_query* q, uint32_t* offsets, uint32_t* neighbors, uint32_t* labels);
@@ -162,6 +170,13 @@ void smx_enum_opts_default(smx_enum_opts* o);
  * mapped) is polled by the device; setting it non-zero ends the run with SMX_STOPPED. */
 int smx_enumerate(smx_graph* g, const smx_query* q, const smx_cand* c, const uint32_t* order,
                   const smx_enum_opts* opts, uint64_t limit, volatile uint32_t* stop, smx_stats* out);
+
+/* Stop word for smx_enumerate: pinned, device-mapped host memory holding one
+ * uint32 (initially 0); the counterpart of the reference's
+ * std::atomic<bool> stop_flag (explore.h:600-602).  Another host thread sets
+ * *flag = 1 to end a running enumeration with SMX_STOPPED. */
+int smx_stop_flag_create(int device, volatile uint32_t** flag);
+void smx_stop_flag_destroy(volatile uint32_t* flag);
 
 /* ------------------------------------------------------------ batched enumeration */
 /* Many queries against one data graph in one persistent work-stealing launch,

@@ -29,7 +29,7 @@ from . import _lib
 from ._lib import SmxError, check, lib
 
 __all__ = [
-    "Graph", "Query", "CandidateParam", "Edges", "Config", "EnumOptions", "Stats",
+    "Graph", "Query", "CandidateParam", "StopFlag", "Edges", "Config", "EnumOptions", "Stats",
     "Filter_NLF", "Filter_GQL", "Order_RI", "Order_GQL", "isValid", "explore",
     "explore_Intersection_Recursive", "explore_Intersection_Cache_DAF_Filter", "explore_batch",
     "SmxError", "device_count", "NLF", "GQL", "EXPLORE_CANDIDATES", "EXPLORE_CACHE_DAF",
@@ -393,13 +393,39 @@ def explore(data: Graph, query: Query, can: CandidateParam, order=None, opts: En
     o = opts.to_c()
     st = _lib.StatsC()
     ord_arr = None if order is None else np.ascontiguousarray(order, dtype=np.uint32)
+    stop_ptr = stop.ptr if isinstance(stop, StopFlag) else stop
     rc = lib.smx_enumerate(data._h, query._h, can._h, None if ord_arr is None else _p32(ord_arr), ctypes.byref(o),
-                           output_limit, stop, ctypes.byref(st))
+                           output_limit, stop_ptr, ctypes.byref(st))
     if rc not in (_lib.SMX_OK, _lib.SMX_TIMEOUT, _lib.SMX_STOPPED):
         check(rc)
     out = Stats.from_c(st)
     out.status = rc
     return out
+
+
+class StopFlag:
+    """Pinned, device-mapped stop word (smx_stop_flag_create): the reference's
+    std::atomic<bool> stop_flag.  ``set()`` from any host thread ends a running
+    explore() with status SMX_STOPPED and a partial count."""
+
+    def __init__(self, device: int = 0):
+        self._p = _u32p()
+        check(lib.smx_stop_flag_create(device, ctypes.byref(self._p)))
+
+    def set(self, value: int = 1) -> None:
+        self._p[0] = value
+
+    def clear(self) -> None:
+        self._p[0] = 0
+
+    @property
+    def ptr(self):
+        return self._p
+
+    def __del__(self):
+        if getattr(self, "_p", None) and lib is not None:
+            lib.smx_stop_flag_destroy(self._p)
+            self._p = None
 
 
 def explore_Intersection_Recursive(data: Graph, query: Query, order, cfg: Config, output_limit: int = 0,

@@ -77,6 +77,9 @@ SIGNATURES = [
     ("smx_status_str", ctypes.c_char_p, [_i32]),
     ("smx_last_error", ctypes.c_char_p, []),
     ("smx_device_count", _i32, []),
+    ("smx_mark_begin", _i32, [_vp]),
+    ("smx_mark_end", _i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("smx_launch_count", _u64, []),
     ("smx_graph_create", _i32, [_pu64, _pu32, _pu32, _u32, _u64, _i32, _pvp]),
     ("smx_graph_load_text", _i32, [_str, _i32, _pvp]),
     ("smx_graph_generate", _i32, [_u32, _u64, _dbl, _u32, _dbl, _u64, _i32, _pvp]),
@@ -104,6 +107,8 @@ SIGNATURES = [
     ("smx_cand_destroy", None, [_vp]),
     ("smx_enum_opts_default", None, [ctypes.POINTER(EnumOpts)]),
     ("smx_enumerate", _i32, [_vp, _vp, _vp, _pu32, ctypes.POINTER(EnumOpts), _u64, _pu32, ctypes.POINTER(StatsC)]),
+    ("smx_stop_flag_create", _i32, [_i32, ctypes.POINTER(_pu32)]),
+    ("smx_stop_flag_destroy", None, [_pu32]),
     ("smx_enumerate_batch", _i32, [_vp, _pvp, _pvp, ctypes.POINTER(_pu32), _u32, ctypes.POINTER(EnumOpts), _u64,
                                    _pu64, ctypes.POINTER(StatsC)]),
 ]

@@ -13,6 +13,10 @@
 
 using namespace smx;
 
+namespace smx {
+uint64_t launch_count();
+}
+
 namespace {
 int check_device(int device) {
     if (device < 0) return SMX_OK;  // host-only graph
@@ -72,6 +76,27 @@ int smx_device_count(void) {
     }
     return n;
 }
+
+int smx_mark_begin(smx_graph* g) {
+    if (!g || g->device < 0) return fail(SMX_BAD_ARGUMENT, "needs a device graph");
+    SMX_CUDA_TRY(cudaSetDevice(g->device));
+    for (auto& e : g->mark)
+        if (!e) SMX_CUDA_TRY(cudaEventCreate(&e));
+    SMX_CUDA_TRY(cudaEventRecord(g->mark[0], g->stream));
+    return SMX_OK;
+}
+
+int smx_mark_end(smx_graph* g, double* ms) {
+    if (!g || !ms || !g->mark[0]) return fail(SMX_BAD_ARGUMENT, "smx_mark_begin first");
+    SMX_CUDA_TRY(cudaEventRecord(g->mark[1], g->stream));
+    SMX_CUDA_TRY(cudaEventSynchronize(g->mark[1]));
+    float f = 0;
+    SMX_CUDA_TRY(cudaEventElapsedTime(&f, g->mark[0], g->mark[1]));
+    *ms = f;
+    return SMX_OK;
+}
+
+uint64_t smx_launch_count(void) { return launch_count(); }
 
 // ------------------------------------------------------------------ graphs
 
@@ -171,6 +196,8 @@ void smx_graph_destroy(smx_graph* g) {
     cudaFree(g->d_lab);
     cudaFree(g->d_hist);
     cudaFree(g->d_scratch);
+    for (auto& e : g->mark)
+        if (e) cudaEventDestroy(e);
     if (g->stream) cudaStreamDestroy(g->stream);
     delete g;
 }
@@ -424,6 +451,24 @@ int smx_enumerate(smx_graph* g, const smx_query* q, const smx_cand* c, const uin
     std::vector<uint64_t> lim{limit};
     uint64_t count = 0;
     return device_enumerate(g, qs, cs, os, o, lim, stop, &count, out, false);
+}
+
+int smx_stop_flag_create(int device, volatile uint32_t** flag) {
+    if (!flag) return fail(SMX_BAD_ARGUMENT, "null argument");
+    *flag = nullptr;
+    int rc = check_device(device);
+    if (rc != SMX_OK) return rc;
+    if (device < 0) return fail(SMX_BAD_ARGUMENT, "a stop word needs a device");
+    SMX_CUDA_TRY(cudaSetDevice(device));
+    void* p = nullptr;
+    SMX_CUDA_TRY(cudaHostAlloc(&p, 64, cudaHostAllocMapped | cudaHostAllocPortable));
+    std::memset(p, 0, 64);
+    *flag = static_cast<volatile uint32_t*>(p);
+    return SMX_OK;
+}
+
+void smx_stop_flag_destroy(volatile uint32_t* flag) {
+    if (flag) cudaFreeHost((void*)flag);
 }
 
 int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand* const* cs,

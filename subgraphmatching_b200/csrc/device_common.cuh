@@ -7,8 +7,12 @@
 // Kernel launches and shared-memory declarations go through these macros so
 // the same kernel sources also build for the CPU warp emulator that the test
 // suite uses (tests/emu, -DSMX_EMU); the CUDA build expands them to plain CUDA.
+namespace smx {
+void note_launch();  // counts launches for smx_launch_count()
+}
 #ifndef SMX_EMU
-#define SMX_LAUNCH(kernel, grid, block, smem, stream, ...) kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__)
+#define SMX_LAUNCH(kernel, grid, block, smem, stream, ...) \
+    (::smx::note_launch(), kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__))
 #define SMX_EXTERN_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
 #define SMX_SHARED_ARRAY(type, name, count) __shared__ type name[count]
 #endif

@@ -262,6 +262,8 @@ __device__ void check_global_stop(const EnumArgs& A, uint64_t deadline) {
 struct Tally {
     unsigned long long local = 0;
     uint32_t q = 0;
+    uint32_t polls = 0;
+    uint64_t deadline = 0;
 };
 
 __device__ __forceinline__ void flush_tally(const EnumArgs& A, Tally& T) {
@@ -273,9 +275,12 @@ __device__ __forceinline__ void flush_tally(const EnumArgs& A, Tally& T) {
     __syncwarp();
 }
 
-// Periodic in-task check: abort flag, the query's limit, large local tallies.
+// Periodic in-task check: abort flag, the query's limit, large local tallies;
+// every 64th call also the caller's stop word and the time budget, so a long
+// subtree notices them too.
 __device__ __forceinline__ bool task_should_stop(const EnumArgs& A, Tally& T) {
     if (T.local > (1ull << 22)) flush_tally(A, T);
+    if ((++T.polls & 63u) == 0) check_global_stop(A, T.deadline);
     const bool a = poll_abort(A);
     const bool b = query_stopped(A, T.q);
     return a || b;
@@ -297,14 +302,17 @@ __device__ __forceinline__ Row table_row(const BnRef& r, uint32_t idx) {
 // copy), otherwise the intersection of all rows, shortest first, in the
 // depth's scratch buffer.  For the last depth (COUNT_ONLY) returns
 // |intersection| and leaves the two lists that define it in r0 / r1 for the
-// conflict test.
+// conflict test.  Rows of the backward neighbour at skip_depth are left out;
+// with no row left the result is "unconstrained" (returns kInvalid).
 template <bool COUNT_ONLY>
 __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr, Stage& st, uint32_t gallop_ratio,
-                               Counters& C, Row& r0, Row& r1, const uint32_t (&slot_idx)[2]) {
+                               Counters& C, Row& r0, Row& r1, const uint32_t (&slot_idx)[2],
+                               uint32_t skip_depth = kInvalid) {
     const uint32_t lane = lane_id();
     const uint32_t nb = D.nbn;
     // lane i < min(nb, 32) holds row i
     Row mine{nullptr, 0xffffffffu};
+    bool mine_ok = false;
     {
         uint32_t bd = 0;
         BnRef R{};
@@ -314,18 +322,25 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
         }
         const uint32_t id_lo = __shfl_sync(kFull, slot_idx[0], bd & 31);
         const uint32_t id_hi = __shfl_sync(kFull, slot_idx[1], bd & 31);
-        if (lane < nb) mine = table_row(R, bd < 32 ? id_lo : id_hi);
+        if (lane < nb && bd != skip_depth) {
+            mine = table_row(R, bd < 32 ? id_lo : id_hi);
+            mine_ok = true;
+        }
     }
-    if (nb == 1) {
-        r0 = Row{reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(mine.p), 0)),
-                 __shfl_sync(kFull, mine.len, 0)};
-        r1 = Row{nullptr, 0};
-        return r0.len;
+    const uint32_t avail0 = __ballot_sync(kFull, mine_ok);
+    uint32_t extra = 0;  // rows beyond the first 32 (queries with more than 33 vertices)
+    for (uint32_t i = 32; i < nb; ++i) extra += (P.bn[D.bn_begin + i].depth != skip_depth);
+    const uint32_t nrows = __popc(avail0);
+    const uint32_t total = nrows + extra;
+    r1 = Row{nullptr, 0};
+    if (total == 0) {
+        r0 = Row{nullptr, 0};
+        return kInvalid;
     }
     // order rows by length: repeatedly take the shortest unused one
-    uint32_t used = 0;  // bit per lane
+    uint32_t used = ~avail0;  // bit per lane
     auto take_shortest = [&](Row& out) {
-        const bool avail = lane < nb && !((used >> lane) & 1u);
+        const bool avail = !((used >> lane) & 1u);
         const uint32_t key = avail ? mine.len : 0xffffffffu;
         const uint32_t mn = __reduce_min_sync(kFull, key);
         const uint32_t who = __ffs(__ballot_sync(kFull, avail && key == mn)) - 1;
@@ -333,13 +348,16 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
         out.p = reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(mine.p), who));
         out.len = __shfl_sync(kFull, mine.len, who);
     };
-    const uint32_t nrows = min(nb, 32u);
     Row a, b;
     take_shortest(a);
+    if (total == 1) {
+        r0 = a;
+        return a.len;
+    }
     take_shortest(b);
     C.isect++;
     C.bytes += 4ull * (a.len + b.len);
-    if (nrows == 2 && nb <= 32) {
+    if (total == 2) {
         if (COUNT_ONLY) {
             r0 = a;
             r1 = b;
@@ -347,7 +365,6 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
         }
         const uint32_t k = isect<false>(st, gallop_ratio, a.p, a.len, b.p, b.len, scr);
         r0 = Row{scr, k};
-        r1 = Row{nullptr, 0};
         return k;
     }
     // three or more rows: materialise all but the longest, then count with it
@@ -357,12 +374,11 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
         take_shortest(c);
         if (k == 0) {
             r0 = Row{scr, 0};
-            r1 = Row{nullptr, 0};
             return 0;
         }
         C.isect++;
         C.bytes += 4ull * (k + c.len);
-        const bool last = (t + 1 == nrows) && nb <= 32;
+        const bool last = (t + 1 == nrows) && extra == 0;
         if (last && COUNT_ONLY) {
             r0 = Row{scr, k};
             r1 = c;
@@ -374,6 +390,7 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
     // backward neighbours beyond 32 (queries with more than 33 vertices): in input order
     for (uint32_t i = 32; i < nb; ++i) {
         const BnRef R = P.bn[D.bn_begin + i];
+        if (R.depth == skip_depth) continue;
         const uint32_t id = __shfl_sync(kFull, R.depth < 32 ? slot_idx[0] : slot_idx[1], R.depth & 31);
         const Row c = table_row(R, id);
         if (k == 0) break;
@@ -391,8 +408,146 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
         }
     }
     r0 = Row{scr, k};
-    r1 = Row{nullptr, 0};
     return k;
+}
+
+// Per-lane |a ∩ b| of two sorted lists: walks the shorter one and narrows a
+// binary search in the longer one (no warp collectives; lanes run
+// independently on their own lists).
+__device__ __forceinline__ uint32_t lane_isect_count(const uint32_t* a, uint32_t na, const uint32_t* b,
+                                                     uint32_t nb) {
+    if (na > nb) {
+        const uint32_t* t = a;
+        a = b;
+        b = t;
+        const uint32_t tn = na;
+        na = nb;
+        nb = tn;
+    }
+    uint32_t cnt = 0, lo = 0;
+    for (uint32_t i = 0; i < na && lo < nb; ++i) {
+        const uint32_t x = a[i];
+        uint32_t l = lo, h = nb;
+        while (l < h) {
+            const uint32_t m = (l + h) >> 1;
+            if (b[m] < x) l = m + 1; else h = m;
+        }
+        lo = l;
+        if (lo < nb && b[lo] == x) {
+            ++cnt;
+            ++lo;
+        }
+    }
+    return cnt;
+}
+
+// The part of the last depth L = n-1 that does not depend on the candidate
+// chosen at depth n-2, computed once when depth n-2 is opened:
+//   G      intersection of the rows of L's backward neighbours other than n-2
+//          (unconstrained if n-2 is the only one);
+//   prank  per lane j < n-2: the index in C(u_L) of the embedded vertex of
+//          depth j if it is a candidate of u_L inside G, else kInvalid;
+//   K0     |G| - #valid pranks (the count when n-2 is not a backward neighbour).
+// Then every candidate of depth n-2 is counted by its own lane (leaf_batch).
+struct LeafState {
+    uint64_t gptr;
+    uint32_t glen;
+    uint32_t gany;
+    uint32_t inb;      // n-2 is a backward neighbour of L
+    uint32_t k0;
+    BnRef row;         // E[u_{n-2}][u_L] when inb
+    uint32_t prank0, prank1;
+    uint64_t pmask;    // depths with a valid prank
+};
+
+__device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, uint32_t gallop_ratio, Counters& C,
+                             const uint32_t (&slot_idx)[2], const uint32_t (&slot_vid)[2], LeafState& S) {
+    const uint32_t lane = lane_id();
+    const uint32_t L = P.n - 1;
+    const DepthInfo& D = P.dep[L];
+    Row r0, r1;
+    const uint32_t g = build_rows<false>(P, D, scr + D.scr_off, st, gallop_ratio, C, r0, r1, slot_idx, L - 1);
+    S.gany = g != kInvalid;
+    S.gptr = reinterpret_cast<uint64_t>(r0.p);
+    S.glen = S.gany ? g : 0;
+    S.inb = 0;
+    for (uint32_t i = 0; i < D.nbn; ++i) {
+        const BnRef R = P.bn[D.bn_begin + i];
+        if (R.depth == L - 1) {
+            S.inb = 1;
+            S.row = R;
+        }
+    }
+    uint64_t pm = 0;
+    for (uint32_t half = 0; half < 2; ++half) {
+        const uint32_t j = half * 32 + lane;
+        uint32_t pr = kInvalid;
+        if (j + 1 < L) {  // depths 0 .. n-3
+            const uint32_t w = half ? slot_vid[1] : slot_vid[0];
+            if ((__ldg(P.mask + w) >> D.u) & 1ull) {
+                const uint32_t r = cand_rank(P.rank, P.qn, D.u, w);
+                if (!S.gany || bsearch_global(r0.p, S.glen, r)) pr = r;
+            }
+        }
+        if (half) S.prank1 = pr; else S.prank0 = pr;
+        pm |= (uint64_t)__ballot_sync(kFull, pr != kInvalid) << (32 * half);
+        if (L <= 33) {
+            if (!half) S.prank1 = kInvalid;
+            break;
+        }
+    }
+    S.pmask = pm;
+    S.k0 = S.glen - __popcll(pm);
+}
+
+// Counts the last depth for every valid candidate of the current depth-(n-2)
+// batch at once, one candidate per lane.
+__device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_t* lp, uint32_t base, uint32_t vm,
+                               Counters& C) {
+    const uint32_t lane = lane_id();
+    const uint32_t L = P.n - 1;
+    const uint32_t u = P.dep[L].u;
+    const bool mine = (vm >> lane) & 1u;
+    uint64_t cnt = 0;
+    uint32_t row_len = 0;
+    const uint32_t* row = nullptr;
+    if (mine) {
+        const uint32_t c = lp[base + lane];
+        if (!S.inb) {
+            const uint32_t v = __ldg(P.dep[L - 1].cand + c);
+            uint32_t hit = 0;
+            if ((__ldg(P.mask + v) >> u) & 1ull)
+                hit = bsearch_global(reinterpret_cast<const uint32_t*>(S.gptr), S.glen,
+                                     cand_rank(P.rank, P.qn, u, v));
+            cnt = S.k0 - hit;
+        } else {
+            const Row r = table_row(S.row, c);
+            row = r.p;
+            row_len = r.len;
+            cnt = S.gany ? lane_isect_count(r.p, r.len, reinterpret_cast<const uint32_t*>(S.gptr), S.glen) : r.len;
+        }
+    }
+    if (S.inb) {
+        // fixed embedded vertices inside G that also lie in this lane's row
+        uint64_t pm = S.pmask;
+        while (pm) {
+            const int j = __ffsll((long long)pm) - 1;
+            pm &= pm - 1;
+            const uint32_t r = __shfl_sync(kFull, j < 32 ? S.prank0 : S.prank1, j & 31);
+            if (mine && bsearch_global(row, row_len, r)) --cnt;
+        }
+        C.bytes += mine ? 8ull + 4ull * row_len : 0ull;
+    }
+    // warp sum
+    uint32_t lo = (uint32_t)cnt, hi = (uint32_t)(cnt >> 32);
+    for (int o = 16; o; o >>= 1) {
+        const uint32_t l2 = __shfl_down_sync(kFull, lo, o);
+        const uint32_t h2 = __shfl_down_sync(kFull, hi, o);
+        const uint64_t s = ((uint64_t)hi << 32 | lo) + ((uint64_t)h2 << 32 | l2);
+        lo = (uint32_t)s;
+        hi = (uint32_t)(s >> 32);
+    }
+    return __shfl_sync(kFull, (uint64_t)hi << 32 | lo, 0);
 }
 
 // Full-warp count of the last depth L for the current prefix (depths < L set).
@@ -464,6 +619,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
 #define vid0 slot_vid[0]
 #define vid1 slot_vid[1]
     uint32_t d = 2;
+    LeafState leaf;
     auto open_depth = [&](uint32_t dd) {
         Row r0, r1;
         const DepthInfo& D = P.dep[dd];
@@ -472,6 +628,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(len, dd, k);
         SLOT_SET(pos, dd, 0u);
         SLOT_SET(vm, dd, 0u);
+        if (dd + 2 == n && k) leaf_prepare(P, scr, st, A.gallop_ratio, C, slot_idx, slot_vid, leaf);
     };
     open_depth(2);
     uint32_t iter = 0;
@@ -499,6 +656,15 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
             SLOT_SET(vm, d, vm);
             continue;
         }
+        if (d + 2 == n) {
+            // all valid candidates of this batch at once, one per lane
+            const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+            const uint32_t base = SLOT_GET(pos, d) - 32;
+            local += leaf_batch(P, leaf, lp, base, vm, C);
+            C.nodes += __popc(vm);
+            SLOT_SET(vm, d, 0u);
+            continue;
+        }
         const uint32_t b = __ffs(vm) - 1;
         SLOT_SET(vm, d, vm & (vm - 1));
         const uint32_t pos = SLOT_GET(pos, d) - 32 + b;
@@ -508,10 +674,6 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(idx, d, c);
         SLOT_SET(vid, d, v);
         C.nodes++;
-        if (d + 2 == n) {
-            local += last_depth_count(P, n - 1, scr, st, A.gallop_ratio, C, slot_idx, slot_vid);
-            continue;
-        }
         ++d;
         open_depth(d);
     }
@@ -779,6 +941,7 @@ __global__ void __launch_bounds__(256) enum_kernel(EnumArgs A) {
     const uint64_t deadline = A.budget_ns ? global_timer_ns() + A.budget_ns : 0;
     Counters C;
     Tally T;
+    T.deadline = deadline;
     const uint64_t total = A.task_prefix[A.nq];
     uint32_t q = 0;
     uint64_t qlo = A.task_prefix[0], qhi = A.task_prefix[1];
@@ -875,7 +1038,8 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
         D.bn_begin = (uint32_t)hb.bn.size();
         D.anc = anc[dd];
         D.iter_op = kInvalid;
-        uint32_t cap = 0xffffffffu;
+        uint32_t cap = 0xffffffffu;       // result <= min over all rows
+        uint32_t cap_other = 0xffffffffu; // the last depth's G leaves out depth n-2's row
         for (uint32_t p : bnd[dd]) {
             BnRef r{};
             r.depth = p;
@@ -889,6 +1053,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                 r.edge = T.d_edge;
                 r.max_deg = T.max_deg;
                 cap = std::min(cap, T.max_deg);
+                if (p + 2 != n || dd + 1 != n) cap_other = std::min(cap_other, T.max_deg);
             }
             hb.bn.push_back(r);
         }
@@ -896,6 +1061,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
         if (mode == SMX_EXPLORE_CANDIDATES && dd >= 2 && D.nbn >= 2) {
             D.scr_off = (uint32_t)scr;
             // result <= min row <= cap; a second cap for the >32-neighbour swap
+            if (dd + 1 == n && cap_other != 0xffffffffu) cap = std::max(cap, cap_other);
             const uint64_t need = (uint64_t)cap * (D.nbn > 32 ? 2 : 1);
             scr += (need + 8 + 3) & ~3ull;  // 16-byte aligned buffers
         }

@@ -2,6 +2,7 @@
 // utilities, the static orders and the intersection plan.  Device code lives
 // in filter.cu / enumerate.cu; the C ABI in capi.cpp.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -67,6 +68,12 @@ struct Alias {
     }
 };
 }  // namespace
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 const std::string& last_error() { return g_last_error; }
@@ -320,60 +327,95 @@ void query_from_host_graph(const HostGraph& g, HostQuery& q) {
     q.finish();
 }
 
-// Random-walk query extraction.  The walk starts at a seeded vertex of
-// degree >= 2 and records every vertex in order of first visit until k are
-// seen.  Dense: the induced subgraph on those vertices; retried with new
-// starts until the average degree exceeds 3 (the densest attempt wins if none
-// does).  Sparse: only the edges the walk traversed.
+// Seeded query extraction.
+//   Sparse: a random walk from a seeded vertex of degree >= 2 records every
+//   vertex in order of first visit until k are seen; the query holds only the
+//   edges the walk traversed (a tree plus the walk's repeat crossings).
+//   Dense: from a seeded start vertex the set grows one vertex at a time,
+//   taking among the set's neighbours (hub rows sampled to 64 entries) the one
+//   with the most links into the set (ties broken at random); the query is
+//   the induced subgraph.  Retried from new starts until the average degree
+//   exceeds 3 (the densest attempt wins otherwise).
+// Query vertex ids follow the order in which vertices joined; labels are
+// inherited from the data graph.
+namespace {
+bool adjacent(const HostGraph& g, uint32_t a, uint32_t b) {
+    return std::binary_search(g.adj.begin() + g.off[a], g.adj.begin() + g.off[a + 1], b);
+}
+}  // namespace
+
 bool generate_walk_query(const HostGraph& g, uint32_t k, bool dense, uint64_t seed, HostQuery& q) {
     if (k == 0 || k > kMaxQ || g.n == 0) return false;
     Rng rng(seed ^ 0x5bd1e9955bd1e995ull);
     std::vector<uint32_t> best_vs;
     std::vector<std::pair<uint32_t, uint32_t>> best_es;
     double best_avg = -1.0;
-    const int attempts = dense ? 64 : 16;
+    const int attempts = dense ? 48 : 16;
     for (int att = 0; att < attempts; ++att) {
         uint32_t start = 0;
         for (int t = 0; t < 1000; ++t) {
             start = (uint32_t)rng.below(g.n);
-            if (g.deg(start) >= 2) break;
+            if (g.deg(start) >= (dense ? 3u : 2u)) break;
         }
         std::vector<uint32_t> vs{start};
-        std::vector<std::pair<uint32_t, uint32_t>> walked;
+        std::vector<std::pair<uint32_t, uint32_t>> es;
         auto idx_of = [&](uint32_t v) -> int {
             for (size_t i = 0; i < vs.size(); ++i)
                 if (vs[i] == v) return (int)i;
             return -1;
         };
-        uint32_t cur = start;
-        uint64_t steps = 0;
-        while (vs.size() < k && steps < 100000ull * k) {
-            ++steps;
-            uint32_t d = g.deg(cur);
-            if (d == 0) break;
-            uint32_t nxt = g.adj[g.off[cur] + rng.below(d)];
-            int a = idx_of(cur), b = idx_of(nxt);
-            if (b < 0) {
-                vs.push_back(nxt);
-                b = (int)vs.size() - 1;
+        if (!dense) {
+            uint32_t cur = start;
+            uint64_t steps = 0;
+            while (vs.size() < k && steps < 100000ull * k) {
+                ++steps;
+                uint32_t d = g.deg(cur);
+                if (d == 0) break;
+                uint32_t nxt = g.adj[g.off[cur] + rng.below(d)];
+                int a = idx_of(cur), b = idx_of(nxt);
+                if (b < 0) {
+                    vs.push_back(nxt);
+                    b = (int)vs.size() - 1;
+                }
+                uint32_t x = (uint32_t)std::min(a, b), y = (uint32_t)std::max(a, b);
+                if (x != y && std::find(es.begin(), es.end(), std::make_pair(x, y)) == es.end()) es.emplace_back(x, y);
+                cur = nxt;
             }
-            uint32_t x = (uint32_t)std::min(a, b), y = (uint32_t)std::max(a, b);
-            if (x != y && std::find(walked.begin(), walked.end(), std::make_pair(x, y)) == walked.end())
-                walked.emplace_back(x, y);
-            cur = nxt;
+        } else {
+            while (vs.size() < k) {
+                std::vector<uint32_t> cand;
+                for (uint32_t v : vs) {
+                    const uint32_t d = g.deg(v);
+                    if (d <= 64) {
+                        for (uint64_t e = g.off[v]; e < g.off[v + 1]; ++e) cand.push_back(g.adj[e]);
+                    } else {
+                        for (int t = 0; t < 64; ++t) cand.push_back(g.adj[g.off[v] + rng.below(d)]);
+                    }
+                }
+                std::sort(cand.begin(), cand.end());
+                cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+                uint32_t best = kInvalid, best_links = 0, ties = 0;
+                for (uint32_t w : cand) {
+                    if (idx_of(w) >= 0) continue;
+                    uint32_t links = 0;
+                    for (uint32_t v : vs) links += adjacent(g, w, v);
+                    if (best == kInvalid || links > best_links) {
+                        best = w;
+                        best_links = links;
+                        ties = 1;
+                    } else if (links == best_links && rng.below(++ties) == 0) {
+                        best = w;
+                    }
+                }
+                if (best == kInvalid) break;
+                vs.push_back(best);
+            }
+            if (vs.size() == k)
+                for (uint32_t i = 0; i < k; ++i)
+                    for (uint32_t j = i + 1; j < k; ++j)
+                        if (adjacent(g, vs[i], vs[j])) es.emplace_back(i, j);
         }
         if (vs.size() < k) continue;
-        std::vector<std::pair<uint32_t, uint32_t>> es;
-        if (dense) {
-            for (uint32_t i = 0; i < k; ++i)
-                for (uint32_t j = i + 1; j < k; ++j) {
-                    uint32_t a = vs[i], b = vs[j];
-                    if (std::binary_search(g.adj.begin() + g.off[a], g.adj.begin() + g.off[a + 1], b))
-                        es.emplace_back(i, j);
-                }
-        } else {
-            es = walked;
-        }
         double avg = 2.0 * es.size() / k;
         if (avg > best_avg) {
             best_avg = avg;
@@ -386,7 +428,10 @@ bool generate_walk_query(const HostGraph& g, uint32_t k, bool dense, uint64_t se
     std::sort(best_es.begin(), best_es.end());
     q.n = k;
     std::vector<uint32_t> deg(k, 0);
-    for (auto& e : best_es) { deg[e.first]++; deg[e.second]++; }
+    for (auto& e : best_es) {
+        deg[e.first]++;
+        deg[e.second]++;
+    }
     q.off.assign(k + 1, 0);
     for (uint32_t i = 0; i < k; ++i) q.off[i + 1] = q.off[i] + deg[i];
     q.adj.assign(q.off[k], 0);

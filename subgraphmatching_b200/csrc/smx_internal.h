@@ -104,6 +104,7 @@ struct smx_graph {
     // scratch reused across calls
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
+    cudaEvent_t mark[2] = {nullptr, nullptr};
 };
 
 struct smx_query {

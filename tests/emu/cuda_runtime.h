@@ -152,8 +152,11 @@ void launch(void (*k)(P...), dim3 grid, dim3 block, size_t smem, A&&... args) {
 #define blockDim (::emu::ctx.bdim)
 #define gridDim (::emu::ctx.gdim)
 
+namespace smx {
+void note_launch();
+}
 #define SMX_LAUNCH(kernel, grid, block, smem, stream, ...) \
-    ::emu::launch(kernel, dim3(grid), dim3(block), (size_t)(smem), __VA_ARGS__)
+    (::smx::note_launch(), ::emu::launch(kernel, dim3(grid), dim3(block), (size_t)(smem), __VA_ARGS__))
 #define SMX_EXTERN_SMEM(name) unsigned char* name = ::emu::ctx.blk->dyn.data()
 #define SMX_SHARED_ARRAY(type, name, count) type* name = ::emu::shared_static<type>(__LINE__, (count))
 
@@ -294,6 +297,10 @@ cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t a, cudaEvent_t b);
 cudaError_t cudaGetLastError();
 const char* cudaGetErrorString(cudaError_t e);
 cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned flags);
+#define cudaHostAllocMapped 2
+#define cudaHostAllocPortable 1
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned flags);
+cudaError_t cudaFreeHost(void* p);
 cudaError_t cudaStreamBeginCapture(cudaStream_t s, cudaStreamCaptureMode m);
 cudaError_t cudaStreamEndCapture(cudaStream_t s, cudaGraph_t* g);
 cudaError_t cudaGraphInstantiate(cudaGraphExec_t* e, cudaGraph_t g, unsigned long long flags);

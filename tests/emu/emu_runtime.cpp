@@ -103,6 +103,14 @@ cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned) {
     *d = h;
     return cudaSuccess;
 }
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned) {
+    *p = poisoned_alloc(n);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFreeHost(void* p) {
+    std::free(p);
+    return cudaSuccess;
+}
 cudaError_t cudaStreamBeginCapture(cudaStream_t, cudaStreamCaptureMode) {
     emu::capture().on = true;
     emu::capture().ops.clear();
