@@ -158,13 +158,22 @@ def test_edge_cases(gpu):
     assert smx.explore(dg, q3, can, opts=smx.EnumOptions(explore=1)).count > 0
 
 
-def test_limit_semantics(gpu, port):
+def golden_count(golden, graph, k, seed):
+    for g in golden["graphs"]:
+        if g["name"] == graph:
+            for q in g["queries"]:
+                if q["k"] == k and q["seed"] == seed:
+                    return q["count"]
+    raise KeyError((graph, k, seed))
+
+
+def test_limit_semantics(gpu, golden):
     hg, dg, gpath = device_graph(9500, 35000, 2.5, 1, 1)
     q, qpath = query_file(hg, 5, True, 12)
     can = smx.CandidateParam(dg, q)
     smx.Filter_GQL(dg, q, can)
     full = smx.explore(dg, q, can).count
-    assert full == 33_648_346  # golden (reference) value
+    assert full == golden_count(golden, "cl9500_unlabelled", 5, 12)  # the reference's count
     for lim in (1, 999, full - 1, full, full + 1):
         for mode in (0, 1):
             st = smx.explore(dg, q, can, opts=smx.EnumOptions(explore=mode), output_limit=lim)
@@ -194,21 +203,26 @@ def test_batch_matches_single(gpu):
         assert counts == singles
 
 
-def test_time_budget_returns_partial_count(gpu):
+LONG = ("cl9500_unlabelled", 6, False, 13)  # 28.3 billion embeddings (reference count)
+
+
+def test_time_budget_returns_partial_count(gpu, golden):
     hg, dg, _ = device_graph(9500, 35000, 2.5, 1, 1)
-    q, _ = query_file(hg, 8, True, 15)       # 47.6 billion embeddings
+    q, _ = query_file(hg, LONG[1], LONG[2], LONG[3])
+    full = golden_count(golden, LONG[0], LONG[1], LONG[3])
     can = smx.CandidateParam(dg, q)
     smx.Filter_GQL(dg, q, can)
     t0 = time.time()
     st = smx.explore(dg, q, can, opts=smx.EnumOptions(time_budget_ms=50))
     assert st.status == _lib.SMX_TIMEOUT
-    assert 0 < st.count < 47_613_736_386
+    assert 0 < st.count < full
     assert time.time() - t0 < 30
 
 
-def test_stop_flag_from_another_thread(gpu):
+def test_stop_flag_from_another_thread(gpu, golden):
     hg, dg, _ = device_graph(9500, 35000, 2.5, 1, 1)
-    q, _ = query_file(hg, 8, True, 15)
+    q, _ = query_file(hg, LONG[1], LONG[2], LONG[3])
+    full = golden_count(golden, LONG[0], LONG[1], LONG[3])
     can = smx.CandidateParam(dg, q)
     smx.Filter_GQL(dg, q, can)
     flag = smx.StopFlag(0)
@@ -217,12 +231,23 @@ def test_stop_flag_from_another_thread(gpu):
     st = smx.explore(dg, q, can, stop=flag)
     timer.join()
     assert st.status == _lib.SMX_STOPPED
-    assert 0 < st.count < 47_613_736_386
+    assert 0 < st.count < full
     flag.clear()   # the context stays usable
     q2, _ = query_file(hg, 4, True, 11)
     can2 = smx.CandidateParam(dg, q2)
     smx.Filter_GQL(dg, q2, can2)
-    assert smx.explore(dg, q2, can2, stop=flag).count == 1_400_470
+    assert smx.explore(dg, q2, can2, stop=flag).count == golden_count(golden, "cl9500_unlabelled", 4, 11)
+
+
+def test_large_exhaustive_count(gpu, golden):
+    """28,302,124,178 embeddings, exhaustive, against the reference's count."""
+    hg, dg, _ = device_graph(9500, 35000, 2.5, 1, 1)
+    q, _ = query_file(hg, LONG[1], LONG[2], LONG[3])
+    can = smx.CandidateParam(dg, q)
+    smx.Filter_GQL(dg, q, can)
+    st = smx.explore(dg, q, can, opts=smx.EnumOptions(time_budget_ms=300_000))
+    assert st.status == 0
+    assert st.count == golden_count(golden, LONG[0], LONG[1], LONG[3])
 
 
 def test_scale_invariants(gpu):
