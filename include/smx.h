@@ -68,7 +68,8 @@ typedef struct {
     int32_t bitmap_min;       /* reserved: list length above which a bitmap probe is used (0 = off) */
     int32_t use_tma;          /* stage rows with cp.async.bulk (1) or plain loads (0) */
     int32_t failing_sets;     /* DAF failing-set pruning in SMX_EXPLORE_CACHE_DAF (1 = on) */
-    int32_t reserved0;
+    int32_t lane_depth;       /* candidate-table mode: depth from which each lane enumerates a subtree of
+                                 its own (-1 = chosen from the query, 0 = only the last two depths) */
     double time_budget_ms;    /* 0 = unlimited; on expiry SMX_TIMEOUT with a partial count */
 } smx_enum_opts;
 

@@ -353,13 +353,14 @@ class EnumOptions:
     bitmap_min: int = 0
     use_tma: int = 1
     failing_sets: int = 1
+    lane_depth: int = -1
     time_budget_ms: float = 0.0
 
     def to_c(self):
         o = _lib.EnumOpts()
         lib.smx_enum_opts_default(ctypes.byref(o))
         for k in ("explore", "warps_per_block", "blocks_per_sm", "task_grab", "stage_chunk", "gallop_ratio",
-                  "bitmap_min", "use_tma", "failing_sets"):
+                  "bitmap_min", "use_tma", "failing_sets", "lane_depth"):
             setattr(o, k, int(getattr(self, k)))
         o.time_budget_ms = float(self.time_budget_ms)
         return o

@@ -42,7 +42,7 @@ class EnumOpts(ctypes.Structure):
         ("bitmap_min", ctypes.c_int32),
         ("use_tma", ctypes.c_int32),
         ("failing_sets", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("lane_depth", ctypes.c_int32),
         ("time_budget_ms", ctypes.c_double),
     ]
 

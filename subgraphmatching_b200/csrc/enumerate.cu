@@ -72,7 +72,7 @@ struct QPlan {
     uint32_t nops;
     uint64_t ntasks;
     uint32_t nroot;      // |C(order0)|
-    uint32_t pad;
+    uint32_t lane_depth; // candidate-table mode: from this depth on each lane enumerates its own subtree
     const uint2* rank;
     const uint64_t* mask;
     const uint64_t* off;    // data CSR
@@ -192,6 +192,8 @@ __device__ uint32_t isect(Stage& st, uint32_t gallop_ratio, const uint32_t* S, u
             if (!COUNT_ONLY && f) out[cnt + __popc(b & lanemask_lt())] = x;
             cnt += __popc(b);
         }
+        // callers read the list right away from other lanes
+        __syncwarp();
         return cnt;
     }
     uint32_t sp = 0;
@@ -577,6 +579,161 @@ __device__ uint64_t last_depth_count(const QPlan& P, uint32_t L, uint32_t* scr_b
     return (uint64_t)(k - conflicts);
 }
 
+// ------------------------------------------------------------------ lane-level subtrees
+// Below the plan's lane depth every list is an intersection of table rows and
+// short, so a warp gains nothing from sharing one list: each lane takes one
+// candidate of the batch and enumerates its subtree on its own (a plain
+// depth-first search with no warp collectives).  A depth's candidates are
+// produced by walking its shortest row and probing the others (binary
+// search), so nothing is materialised.
+
+__device__ __forceinline__ Row row_at(const BnRef& r, const uint32_t* idx) {
+    const uint32_t i = idx[r.depth];
+    const uint32_t s = __ldg(r.off + i);
+    return Row{r.edge + s, __ldg(r.off + i + 1) - s};
+}
+
+__device__ __forceinline__ bool in_row(const uint32_t* p, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (__ldg(p + m) < x) lo = m + 1; else hi = m;
+    }
+    return lo < n && __ldg(p + lo) == x;
+}
+
+// x (an index into C(u_d)) lies in every row of depth d except row `skip`.
+__device__ __forceinline__ bool in_other_rows(const QPlan& P, const DepthInfo& D, uint32_t skip, const uint32_t* idx,
+                                              uint32_t x) {
+    for (uint32_t i = 0; i < D.nbn; ++i) {
+        if (i == skip) continue;
+        const Row r = row_at(P.bn[D.bn_begin + i], idx);
+        if (!in_row(r.p, r.len, x)) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ uint32_t shortest_row(const QPlan& P, const DepthInfo& D, const uint32_t* idx, Row& best) {
+    uint32_t bi = 0;
+    best = row_at(P.bn[D.bn_begin], idx);
+    for (uint32_t i = 1; i < D.nbn; ++i) {
+        const Row r = row_at(P.bn[D.bn_begin + i], idx);
+        if (r.len < best.len) {
+            best = r;
+            bi = i;
+        }
+    }
+    return bi;
+}
+
+// Count of the last depth for the lane's prefix: |∩ rows| minus embedded
+// vertices inside it (rl[j] = index of depth j's vertex in C(u_L) or kInvalid).
+__device__ uint64_t lane_leaf(const QPlan& P, const uint32_t* idx, const uint32_t* rl, uint32_t L) {
+    const DepthInfo& D = P.dep[L];
+    Row drv;
+    const uint32_t di = shortest_row(P, D, idx, drv);
+    uint64_t k;
+    if (D.nbn == 1) {
+        k = drv.len;
+    } else {
+        k = 0;
+        for (uint32_t i = 0; i < drv.len; ++i) k += in_other_rows(P, D, di, idx, __ldg(drv.p + i));
+    }
+    if (k == 0) return 0;
+    for (uint32_t j = 0; j < L; ++j) {
+        const uint32_t r = rl[j];
+        if (r != kInvalid && in_row(drv.p, drv.len, r) && (D.nbn == 1 || in_other_rows(P, D, di, idx, r))) --k;
+    }
+    return k;
+}
+
+__device__ __forceinline__ uint32_t rank_in_last(const QPlan& P, uint32_t v) {
+    const uint32_t u = P.dep[P.n - 1].u;
+    return ((__ldg(P.mask + v) >> u) & 1ull) ? cand_rank(P.rank, P.qn, u, v) : kInvalid;
+}
+
+// Stop test for a lane running on its own: the warp-level checks cannot be
+// used there, so the lane reads the flags itself.
+__device__ bool lane_should_stop(const EnumArgs& A, uint32_t q, uint64_t deadline) {
+    if (*reinterpret_cast<volatile int*>(A.status) != 0) return true;
+    if (*reinterpret_cast<volatile uint32_t*>(A.qstop + q) != 0) return true;
+    int code = 0;
+    if (A.host_stop && *A.host_stop) code = SMX_STOPPED;
+    else if (deadline && global_timer_ns() > deadline) code = SMX_TIMEOUT;
+    if (code) {
+        atomicCAS(A.status, 0, code);
+        return true;
+    }
+    return false;
+}
+
+struct LaneWork {
+    unsigned long long nodes = 0, bytes = 0;
+};
+
+// Enumerates depths d0+1 .. n-1 below the lane's candidate at depth d0 (idx,
+// vid, rl hold depths 0 .. d0).  Embeddings found are added to the query's
+// counter in chunks (so a count limit stops other warps early) and the rest
+// is returned.
+__device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0, uint32_t* idx, uint32_t* vid,
+                                 uint32_t* rl, const Tally& T, LaneWork& W) {
+    const uint32_t L = P.n - 1;
+    uint32_t dl[kMaxQ], dp[kMaxQ], db[kMaxQ];
+    const uint32_t* de[kMaxQ];
+    uint64_t cnt = 0;
+    uint32_t d = d0 + 1;
+    auto open = [&](uint32_t dd) {
+        Row r;
+        db[dd] = shortest_row(P, P.dep[dd], idx, r);
+        de[dd] = r.p;
+        dl[dd] = r.len;
+        dp[dd] = 0;
+    };
+    open(d);
+    uint32_t iter = 0;
+    for (;;) {
+        if ((++iter & 1023u) == 0) {
+            if (lane_should_stop(A, T.q, T.deadline)) break;
+            if (cnt >= (1u << 20)) {
+                const unsigned long long tot = atomicAdd(A.qcount + T.q, cnt) + cnt;
+                if (A.qlimit[T.q] && tot >= A.qlimit[T.q]) atomicExch(A.qstop + T.q, 1u);
+                cnt = 0;
+            }
+        }
+        const DepthInfo& D = P.dep[d];
+        bool found = false;
+        uint32_t x = 0, v = 0;
+        while (dp[d] < dl[d]) {
+            x = __ldg(de[d] + dp[d]++);
+            W.bytes += 4;
+            if (D.nbn > 1 && !in_other_rows(P, D, db[d], idx, x)) continue;
+            v = __ldg(D.cand + x);
+            W.bytes += 4;
+            bool clash = false;
+            for (uint32_t j = 0; j < d && !clash; ++j) clash = (vid[j] == v);
+            if (clash) continue;
+            found = true;
+            break;
+        }
+        if (!found) {
+            if (d == d0 + 1) break;
+            --d;
+            continue;
+        }
+        idx[d] = x;
+        vid[d] = v;
+        rl[d] = rank_in_last(P, v);
+        W.nodes++;
+        if (d + 1 == L) {
+            cnt += lane_leaf(P, idx, rl, L);
+            continue;
+        }
+        ++d;
+        open(d);
+    }
+    return cnt;
+}
+
 // One task: root r = row of entry t in E[o0][o1], depth-1 candidate edge[t].
 __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, Stage& st, Counters& C,
                                Tally& T) {
@@ -654,6 +811,39 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
             C.bytes += 8ull * min(32u, len - pos);
             SLOT_SET(pos, d, pos + 32);
             SLOT_SET(vm, d, vm);
+            continue;
+        }
+        if (d >= P.lane_depth && d + 2 < n) {
+            // each lane enumerates the subtree of one candidate of the batch
+            const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
+            const uint32_t base = SLOT_GET(pos, d) - 32;
+            uint32_t lidx[kMaxQ], lvid[kMaxQ], lrl[kMaxQ];
+            const uint32_t my_rl_lo = lane < d ? rank_in_last(P, vid0) : kInvalid;
+            const uint32_t my_rl_hi = lane + 32 < d ? rank_in_last(P, vid1) : kInvalid;
+            for (uint32_t j = 0; j < d; ++j) {
+                lidx[j] = SLOT_GET(idx, j);
+                lvid[j] = SLOT_GET(vid, j);
+                lrl[j] = __shfl_sync(kFull, j < 32 ? my_rl_lo : my_rl_hi, j & 31);
+            }
+            uint64_t mine = 0;
+            LaneWork W;
+            if ((vm >> lane) & 1u) {
+                const uint32_t c = lp[base + lane];
+                lidx[d] = c;
+                lvid[d] = __ldg(P.dep[d].cand + c);
+                lrl[d] = rank_in_last(P, lvid[d]);
+                mine = lane_subtree(A, P, d, lidx, lvid, lrl, T, W);
+            }
+            __syncwarp();
+            for (int o = 16; o; o >>= 1) {
+                mine += __shfl_xor_sync(kFull, mine, o);
+                W.nodes += __shfl_xor_sync(kFull, W.nodes, o);
+                W.bytes += __shfl_xor_sync(kFull, W.bytes, o);
+            }
+            local += mine;
+            C.nodes += __popc(vm) + W.nodes;
+            C.bytes += W.bytes;
+            SLOT_SET(vm, d, 0u);
             continue;
         }
         if (d + 2 == n) {
@@ -998,7 +1188,7 @@ struct HostPlanBuild {
 };
 
 int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order, int mode,
-                    HostPlanBuild& hb) {
+                    int lane_depth, HostPlanBuild& hb) {
     const uint32_t n = q.n;
     std::memset(&hb.plan, 0, sizeof(QPlan));
     QPlan& P = hb.plan;
@@ -1068,6 +1258,22 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
     }
     if (mode == SMX_EXPLORE_CANDIDATES) {
         P.ntasks = n >= 2 ? c->tables[c->tab_index[order[0]][order[1]]].e_cnt : 0;
+        // lane depth: the shallowest depth T >= 2 below which (up to n-2) every
+        // candidate list is an intersection of two or more rows, i.e. short
+        uint32_t T = n >= 2 ? n - 2 : 0;
+        if (lane_depth < 0) {
+            for (uint32_t t = 2; t + 2 < n; ++t) {
+                bool all = true;
+                for (uint32_t e = t + 1; e + 2 <= n; ++e) all &= bnd[e].size() >= 2;
+                if (all) {
+                    T = t;
+                    break;
+                }
+            }
+        } else if (lane_depth >= 2) {
+            T = std::min<uint32_t>((uint32_t)lane_depth, n >= 2 ? n - 2 : 0);
+        }
+        P.lane_depth = T;
     } else {
         Plan plan;
         if (!build_plan(q, order, plan)) return fail(SMX_INVALID_ORDER, "order has a vertex without an earlier neighbour");
@@ -1118,7 +1324,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     uint64_t scratch_elems = 8;
     uint32_t max_ops = 1;
     for (uint32_t i = 0; i < nq; ++i) {
-        int rc = build_host_plan(g, *qs[i], cs[i], orders[i], mode, hb[i]);
+        int rc = build_host_plan(g, *qs[i], cs[i], orders[i], mode, o.lane_depth, hb[i]);
         if (rc != SMX_OK) return rc;
         scratch_elems = std::max(scratch_elems, hb[i].scratch_elems);
         max_ops = std::max(max_ops, hb[i].plan.nops);

@@ -188,6 +188,14 @@ inline T __shfl_down_sync(unsigned, T v, unsigned d) {
     emu::wsync();
     return emu::unpack<T>(y);
 }
+template <class T>
+inline T __shfl_xor_sync(unsigned, T v, int m) {
+    emu::slots()[emu::ctx.lane] = emu::pack(v);
+    emu::wsync();
+    uint64_t y = emu::slots()[(emu::ctx.lane ^ (unsigned)m) & 31];
+    emu::wsync();
+    return emu::unpack<T>(y);
+}
 inline unsigned __ballot_sync(unsigned, int p) {
     emu::slots()[emu::ctx.lane] = p ? 1 : 0;
     emu::wsync();

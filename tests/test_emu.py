@@ -80,3 +80,27 @@ def test_emulated_limit_and_batch(emu, port):
     lim = max(1, refs[big] // 3)
     st = emu.enumerate(dg, qs[big], cs[big], orders[big], explore=0, limit=lim)
     assert st.count == lim and st.limit_reached == 1 and st.raw_count >= lim
+
+
+def test_emulated_lane_subtrees_and_galloping(emu, port):
+    """Per-lane subtree enumeration below the lane depth (chosen from the
+    query, or forced to depth 2) and the galloping intersection (ratio 1, so
+    every long row is probed by binary search) give the oracle's counts."""
+    g, gpath = host_graph(900, 4000, 2.2, 1, 5)
+    off, nb, lab = g.csr()
+    dg = emu.graph(off, nb, lab)
+    gp = port.load_graph(gpath)
+    for k, dense, qseed in [(5, True, 2), (6, True, 3)]:
+        q, qpath = query_file(g, k, dense, qseed)
+        qp = port.load_query(qpath)
+        qo, qn, ql = q.csr()
+        dq = emu.query(qo, qn, ql)
+        c, ok = emu.filter(dg, dq, 1)
+        assert ok
+        order = emu.order_ri(dq, k)
+        ref = port.explore(gp, qp, port.filter(gp, qp, 1), order, 0, 4)[0]
+        assert ref > 0
+        for lane_depth in (-1, 2):
+            assert emu.enumerate(dg, dq, c, order, explore=0, lane_depth=lane_depth).count == ref
+        assert emu.enumerate(dg, dq, c, order, explore=0, lane_depth=0, gallop_ratio=1).count == ref
+        assert emu.enumerate(dg, dq, c, order, explore=1, gallop_ratio=1).count == ref

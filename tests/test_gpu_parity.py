@@ -118,6 +118,27 @@ def test_intersection_modes_agree(gpu, port):
             assert smx.explore(dg, q, can, order, opts).count == ref
 
 
+def test_lane_depths_agree(gpu, golden):
+    """Per-lane subtree enumeration from every possible lane depth (0 = off,
+    -1 = chosen from the query) gives the golden counts, with galloping on and
+    off."""
+    for gcase in golden["graphs"]:
+        hg, dg, _ = device_graph(gcase["n"], gcase["m"], gcase["gamma"], gcase["labels"], gcase["seed"])
+        for qc in gcase["queries"]:
+            if qc["k"] < 5 or (qc["cap"] == 0 and qc["count"] > BIG):
+                continue
+            q, _ = query_file(hg, qc["k"], qc["dense"], qc["seed"])
+            can = smx.CandidateParam(dg, q)
+            if not smx.Filter_GQL(dg, q, can):
+                continue
+            for ld in [-1, 0] + list(range(2, qc["k"] - 1)):
+                for ratio in (16, 1):
+                    opts = smx.EnumOptions(explore=smx.EXPLORE_CANDIDATES, lane_depth=ld, gallop_ratio=ratio)
+                    st = smx.explore(dg, q, can, qc["order_ri"], opts, qc["cap"])
+                    assert st.status == 0
+                    assert st.count == qc["count"], (gcase["name"], qc["k"], qc["seed"], ld, ratio, st.count)
+
+
 def test_edge_cases(gpu):
     hg, dg, _ = device_graph(2000, 9000, 2.5, 4, 3)
     _, _, lab = hg.csr()
