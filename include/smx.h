@@ -61,15 +61,15 @@ typedef enum {
 typedef struct {
     int32_t explore;          /* smx_explore_kind */
     int32_t warps_per_block;  /* 0 = auto (8) */
-    int32_t blocks_per_sm;    /* 0 = auto (occupancy) */
+    int32_t blocks_per_sm;    /* 0 = auto (occupancy); >= 3 also selects a build capped at 80 registers */
     int32_t task_grab;        /* tasks a warp takes per queue access; 0 = auto */
     int32_t stage_chunk;      /* elements per warp staged in shared memory for merge intersection */
     int32_t gallop_ratio;     /* long/short length ratio above which binary-search (galloping) intersection is used */
     int32_t bitmap_min;       /* reserved: list length above which a bitmap probe is used (0 = off) */
     int32_t use_tma;          /* stage rows with cp.async.bulk (1) or plain loads (0) */
     int32_t failing_sets;     /* DAF failing-set pruning in SMX_EXPLORE_CACHE_DAF (1 = on) */
-    int32_t lane_depth;       /* candidate-table mode: depth from which each lane enumerates a subtree of
-                                 its own (-1 = chosen from the query, 0 = only the last two depths) */
+    int32_t lane_depth;       /* candidate-table mode: depth (>= 2) from which each lane enumerates a
+                                 subtree of its own; 0 = off (default), -1 = chosen from the query */
     double time_budget_ms;    /* 0 = unlimited; on expiry SMX_TIMEOUT with a partial count */
 } smx_enum_opts;
 

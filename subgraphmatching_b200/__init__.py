@@ -353,7 +353,7 @@ class EnumOptions:
     bitmap_min: int = 0
     use_tma: int = 1
     failing_sets: int = 1
-    lane_depth: int = -1
+    lane_depth: int = 0
     time_budget_ms: float = 0.0
 
     def to_c(self):

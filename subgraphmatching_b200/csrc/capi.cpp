@@ -419,7 +419,7 @@ void smx_enum_opts_default(smx_enum_opts* o) {
     o->bitmap_min = 0;
     o->use_tma = 1;
     o->failing_sets = 1;
-    o->lane_depth = -1;
+    o->lane_depth = 0;
     o->time_budget_ms = 0;
 }
 

@@ -50,12 +50,29 @@ struct DepthInfo {
     uint32_t u;            // query vertex at this depth
     uint32_t nbn;          // backward neighbours (explore.h: prevNeb[u].size())
     uint32_t bn_begin;     // into QPlan::bn
-    uint32_t scr_off;      // this depth's list buffer in the warp scratch (elements)
+    uint32_t list_off;     // candidate-table mode: buffer holding this depth's list (kInvalid: the row itself)
     uint64_t anc;          // DAF ancestor mask (prune.h:100-104)
     uint32_t nops;         // cache mode: ops computed at this depth
     uint32_t ops_begin;    // into QPlan::op
     uint32_t iter_op;      // cache mode: op holding this depth's candidates
+    uint32_t part_begin;   // candidate-table mode: partial intersections computed at this depth
+    uint32_t npart;
     uint32_t pad;
+};
+
+// Candidate-table mode keeps, for every depth t with backward neighbours
+// p_1 < ... < p_k, the partial intersections P_t^j = row_{p_1} ∩ ... ∩ row_{p_j}
+// (j >= 2) in the warp scratch.  P_t^j is computed at depth p_j, right after
+// the candidate of p_j is chosen, from P_t^{j-1} (still valid: it depends only
+// on depths <= p_{j-1}).  The list of depth t is P_t^k, so a deep depth costs
+// one intersection of a short partial with one row instead of an
+// intersection of all k rows, and an empty partial prunes the candidate at
+// once.  Buffers: word 0 holds the length, the elements start at word 4.
+struct PartRef {
+    uint32_t bn_first;  // BnRef of p_1 (P_t^1 is its row)
+    uint32_t bn_this;   // BnRef of p_j
+    uint32_t prev_off;  // buffer of P_t^{j-1}; kInvalid when j == 2
+    uint32_t out_off;   // buffer of P_t^j
 };
 
 struct OpInfo {
@@ -79,6 +96,13 @@ struct QPlan {
     const uint32_t* adj;
     const BnRef* bn;
     const OpInfo* op;
+    const PartRef* part;
+    // candidate-table mode, last depth L = n-1: its list without the row of
+    // depth n-2 (G) is a row (leaf_g_bn), a partial (leaf_g_off) or unconstrained
+    uint32_t leaf_inb;     // n-2 is a backward neighbour of L
+    uint32_t leaf_g_bn;    // kInvalid unless G is one row
+    uint32_t leaf_g_off;   // kInvalid unless G is a partial buffer
+    uint32_t leaf_gp_off;  // buffer for G without the embedded vertices
     DepthInfo dep[kMaxQ];
 };
 
@@ -413,42 +437,105 @@ __device__ uint32_t build_rows(const QPlan& P, const DepthInfo& D, uint32_t* scr
     return k;
 }
 
-// Per-lane |a ∩ b| of two sorted lists: walks the shorter one and narrows a
-// binary search in the longer one (no warp collectives; lanes run
-// independently on their own lists).
-__device__ __forceinline__ uint32_t lane_isect_count(const uint32_t* a, uint32_t na, const uint32_t* b,
-                                                     uint32_t nb) {
-    if (na > nb) {
-        const uint32_t* t = a;
-        a = b;
-        b = t;
-        const uint32_t tn = na;
-        na = nb;
-        nb = tn;
+// Per-lane |row ∩ G|: row is a table row (read-only), G a sorted list in
+// shared or global memory written by this warp (plain loads).  The shorter
+// list is walked; the longer one is searched.  Searches in a long row run
+// four at a time (independent branch-free searches) so four loads are in
+// flight per step instead of one.
+__device__ __forceinline__ uint32_t lane_count_common(const uint32_t* row, uint32_t nr, const uint32_t* G,
+                                                      uint32_t ng) {
+    if (nr == 0 || ng == 0) return 0;
+    uint32_t cnt = 0;
+    if (nr <= ng) {
+        uint32_t lo = 0;
+        for (uint32_t i = 0; i < nr; ++i) {
+            const uint32_t x = __ldg(row + i);
+            uint32_t l = lo, h = ng;
+            while (l < h) {
+                const uint32_t m = (l + h) >> 1;
+                if (G[m] < x) l = m + 1; else h = m;
+            }
+            lo = l;
+            if (lo == ng) break;
+            cnt += G[lo] == x;
+        }
+        return cnt;
     }
-    uint32_t cnt = 0, lo = 0;
-    for (uint32_t i = 0; i < na && lo < nb; ++i) {
-        const uint32_t x = a[i];
-        uint32_t l = lo, h = nb;
-        while (l < h) {
-            const uint32_t m = (l + h) >> 1;
-            if (b[m] < x) l = m + 1; else h = m;
+    uint32_t lo = 0;  // every later element lies at or after row[lo]
+    for (uint32_t i = 0; i < ng; i += 4) {
+        const uint32_t x0 = G[i];
+        const uint32_t x1 = i + 1 < ng ? G[i + 1] : x0;
+        const uint32_t x2 = i + 2 < ng ? G[i + 2] : x0;
+        const uint32_t x3 = i + 3 < ng ? G[i + 3] : x0;
+        uint32_t b0 = lo, b1 = lo, b2 = lo, b3 = lo, n = nr - lo;
+        while (n > 1) {
+            const uint32_t h = n >> 1;
+            b0 = __ldg(row + b0 + h) <= x0 ? b0 + h : b0;
+            b1 = __ldg(row + b1 + h) <= x1 ? b1 + h : b1;
+            b2 = __ldg(row + b2 + h) <= x2 ? b2 + h : b2;
+            b3 = __ldg(row + b3 + h) <= x3 ? b3 + h : b3;
+            n -= h;
         }
-        lo = l;
-        if (lo < nb && b[lo] == x) {
-            ++cnt;
-            ++lo;
-        }
+        cnt += __ldg(row + b0) == x0;
+        if (i + 1 < ng) cnt += __ldg(row + b1) == x1;
+        if (i + 2 < ng) cnt += __ldg(row + b2) == x2;
+        if (i + 3 < ng) cnt += __ldg(row + b3) == x3;
+        lo = i + 3 < ng ? b3 : lo;
     }
     return cnt;
 }
 
+__device__ __forceinline__ Row part_list(const uint32_t* scr, uint32_t off) {
+    return Row{scr + off + 4, scr[off]};
+}
+
+__device__ __forceinline__ uint32_t slot_get(const uint32_t (&a)[2], uint32_t d) {
+    return __shfl_sync(kFull, d < 32 ? a[0] : a[1], d & 31);
+}
+
+// Computes the partial intersections that end at depth d (its candidate just
+// chosen).  Returns false as soon as one is empty: no embedding extends the
+// candidate.
+__device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& st, uint32_t gallop_ratio,
+                              Counters& C, const uint32_t (&slot_idx)[2]) {
+    const DepthInfo& D = P.dep[d];
+    for (uint32_t i = 0; i < D.npart; ++i) {
+        const PartRef R = P.part[D.part_begin + i];
+        Row a;
+        if (R.prev_off == kInvalid) {
+            const BnRef B = P.bn[R.bn_first];
+            a = table_row(B, slot_get(slot_idx, B.depth));
+        } else {
+            a = part_list(scr, R.prev_off);
+        }
+        const BnRef B2 = P.bn[R.bn_this];
+        const Row b = table_row(B2, slot_get(slot_idx, B2.depth));
+        uint32_t* out = scr + R.out_off;
+        uint32_t k = 0;
+        if (a.len && b.len) {
+            C.isect++;
+            C.bytes += 4ull * (a.len + b.len) + 8;
+            k = a.len <= b.len ? isect<false>(st, gallop_ratio, a.p, a.len, b.p, b.len, out + 4)
+                               : isect<false>(st, gallop_ratio, b.p, b.len, a.p, a.len, out + 4);
+        }
+        __syncwarp();
+        if (lane_id() == 0) out[0] = k;
+        __syncwarp();
+        if (k == 0) return false;
+    }
+    return true;
+}
+
 // The part of the last depth L = n-1 that does not depend on the candidate
-// chosen at depth n-2, computed once when depth n-2 is opened:
-//   G      intersection of the rows of L's backward neighbours other than n-2
-//          (unconstrained if n-2 is the only one);
+// chosen at depth n-2, set up once when depth n-2 is opened:
+//   G      the last depth's list without the row of depth n-2 (a cached
+//          partial, one row, or unconstrained when n-2 is L's only backward
+//          neighbour); when n-2 is a backward neighbour, the embedded vertices
+//          of depths 0 .. n-3 are taken out and the rest is staged in shared
+//          memory when it fits;
 //   prank  per lane j < n-2: the index in C(u_L) of the embedded vertex of
-//          depth j if it is a candidate of u_L inside G, else kInvalid;
+//          depth j if it is a candidate of u_L inside G, else kInvalid (still
+//          needed only where G is unconstrained);
 //   K0     |G| - #valid pranks (the count when n-2 is not a backward neighbour).
 // Then every candidate of depth n-2 is counted by its own lane (leaf_batch).
 struct LeafState {
@@ -462,24 +549,25 @@ struct LeafState {
     uint64_t pmask;    // depths with a valid prank
 };
 
-__device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, uint32_t gallop_ratio, Counters& C,
-                             const uint32_t (&slot_idx)[2], const uint32_t (&slot_vid)[2], LeafState& S) {
+__device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uint32_t (&slot_idx)[2],
+                             const uint32_t (&slot_vid)[2], LeafState& S) {
     const uint32_t lane = lane_id();
     const uint32_t L = P.n - 1;
     const DepthInfo& D = P.dep[L];
-    Row r0, r1;
-    const uint32_t g = build_rows<false>(P, D, scr + D.scr_off, st, gallop_ratio, C, r0, r1, slot_idx, L - 1);
-    S.gany = g != kInvalid;
-    S.gptr = reinterpret_cast<uint64_t>(r0.p);
-    S.glen = S.gany ? g : 0;
-    S.inb = 0;
-    for (uint32_t i = 0; i < D.nbn; ++i) {
-        const BnRef R = P.bn[D.bn_begin + i];
-        if (R.depth == L - 1) {
-            S.inb = 1;
-            S.row = R;
-        }
+    Row G{nullptr, 0};
+    S.gany = 1;
+    if (P.leaf_g_off != kInvalid) {
+        G = part_list(scr, P.leaf_g_off);
+    } else if (P.leaf_g_bn != kInvalid) {
+        const BnRef R = P.bn[P.leaf_g_bn];
+        G = table_row(R, slot_get(slot_idx, R.depth));
+    } else {
+        S.gany = 0;
     }
+    S.gptr = reinterpret_cast<uint64_t>(G.p);
+    S.glen = G.len;
+    S.inb = P.leaf_inb;
+    if (S.inb) S.row = P.bn[D.bn_begin + D.nbn - 1];  // depth n-2 is the last backward neighbour
     uint64_t pm = 0;
     for (uint32_t half = 0; half < 2; ++half) {
         const uint32_t j = half * 32 + lane;
@@ -488,7 +576,7 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, uint32_t 
             const uint32_t w = half ? slot_vid[1] : slot_vid[0];
             if ((__ldg(P.mask + w) >> D.u) & 1ull) {
                 const uint32_t r = cand_rank(P.rank, P.qn, D.u, w);
-                if (!S.gany || bsearch_global(r0.p, S.glen, r)) pr = r;
+                if (!S.gany || bsearch_global(G.p, G.len, r)) pr = r;
             }
         }
         if (half) S.prank1 = pr; else S.prank0 = pr;
@@ -500,10 +588,44 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, uint32_t 
     }
     S.pmask = pm;
     S.k0 = S.glen - __popcll(pm);
+    if (S.inb && S.gany) {
+        // G minus the embedded vertices, into shared memory when it fits (the
+        // stage buffer is idle until depth n-2 is left), else into its buffer;
+        // the cached partial itself stays intact for other prefixes
+        const bool in_smem = G.len <= st.chunk;
+        uint32_t* dst = in_smem ? st.buf : scr + P.leaf_gp_off + 4;
+        uint32_t k = 0;
+        __syncwarp();
+        for (uint32_t base = 0; base < G.len; base += 32) {
+            const uint32_t i = base + lane;
+            uint32_t x = 0;
+            bool keep = false;
+            if (i < G.len) {
+                x = G.p[i];
+                keep = true;
+            }
+            uint64_t m = pm;
+            while (m) {
+                const int j = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                const uint32_t r = __shfl_sync(kFull, j < 32 ? S.prank0 : S.prank1, j & 31);
+                keep &= x != r;
+            }
+            const uint32_t bal = __ballot_sync(kFull, keep);
+            if (keep) dst[k + __popc(bal & lanemask_lt())] = x;
+            k += __popc(bal);
+        }
+        __syncwarp();
+        S.gptr = reinterpret_cast<uint64_t>(dst);
+        S.glen = k;
+        S.pmask = 0;
+        S.k0 = k;
+    }
 }
 
 // Counts the last depth for every valid candidate of the current depth-(n-2)
-// batch at once, one candidate per lane.
+// batch at once, one candidate per lane.  Adds the algorithmic bytes of the
+// whole warp to C.bytes.
 __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_t* lp, uint32_t base, uint32_t vm,
                                Counters& C) {
     const uint32_t lane = lane_id();
@@ -511,7 +633,7 @@ __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_
     const uint32_t u = P.dep[L].u;
     const bool mine = (vm >> lane) & 1u;
     uint64_t cnt = 0;
-    uint32_t row_len = 0;
+    uint32_t row_len = 0, bytes = 0;
     const uint32_t* row = nullptr;
     if (mine) {
         const uint32_t c = lp[base + lane];
@@ -522,15 +644,17 @@ __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_
                 hit = bsearch_global(reinterpret_cast<const uint32_t*>(S.gptr), S.glen,
                                      cand_rank(P.rank, P.qn, u, v));
             cnt = S.k0 - hit;
+            bytes = 16;
         } else {
             const Row r = table_row(S.row, c);
             row = r.p;
             row_len = r.len;
-            cnt = S.gany ? lane_isect_count(r.p, r.len, reinterpret_cast<const uint32_t*>(S.gptr), S.glen) : r.len;
+            cnt = S.gany ? lane_count_common(r.p, r.len, reinterpret_cast<const uint32_t*>(S.gptr), S.glen) : r.len;
+            bytes = 12 + (S.gany ? 4 * (r.len + S.glen) : 0);
         }
     }
-    if (S.inb) {
-        // fixed embedded vertices inside G that also lie in this lane's row
+    if (S.inb && S.pmask) {
+        // unconstrained G: embedded vertices that lie in this lane's row
         uint64_t pm = S.pmask;
         while (pm) {
             const int j = __ffsll((long long)pm) - 1;
@@ -538,18 +662,19 @@ __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_
             const uint32_t r = __shfl_sync(kFull, j < 32 ? S.prank0 : S.prank1, j & 31);
             if (mine && bsearch_global(row, row_len, r)) --cnt;
         }
-        C.bytes += mine ? 8ull + 4ull * row_len : 0ull;
     }
-    // warp sum
+    // warp sums
     uint32_t lo = (uint32_t)cnt, hi = (uint32_t)(cnt >> 32);
     for (int o = 16; o; o >>= 1) {
-        const uint32_t l2 = __shfl_down_sync(kFull, lo, o);
-        const uint32_t h2 = __shfl_down_sync(kFull, hi, o);
+        const uint32_t l2 = __shfl_xor_sync(kFull, lo, o);
+        const uint32_t h2 = __shfl_xor_sync(kFull, hi, o);
         const uint64_t s = ((uint64_t)hi << 32 | lo) + ((uint64_t)h2 << 32 | l2);
         lo = (uint32_t)s;
         hi = (uint32_t)(s >> 32);
+        bytes += __shfl_xor_sync(kFull, bytes, o);
     }
-    return __shfl_sync(kFull, (uint64_t)hi << 32 | lo, 0);
+    C.bytes += bytes;
+    return (uint64_t)hi << 32 | lo;
 }
 
 // Full-warp count of the last depth L for the current prefix (depths < L set).
@@ -559,7 +684,8 @@ __device__ uint64_t last_depth_count(const QPlan& P, uint32_t L, uint32_t* scr_b
     const uint32_t lane = lane_id();
     const DepthInfo& D = P.dep[L];
     Row r0, r1;
-    const uint32_t k = build_rows<true>(P, D, scr_base + D.scr_off, st, gallop_ratio, C, r0, r1, slot_idx);
+    // at most two rows here (n == 3): counted without a buffer
+    const uint32_t k = build_rows<true>(P, D, scr_base, st, gallop_ratio, C, r0, r1, slot_idx);
     if (k == 0) return 0;
     // embedded vertices that are candidates of u_L and lie in the result
     uint32_t conflicts = 0;
@@ -628,10 +754,11 @@ __device__ __forceinline__ uint32_t shortest_row(const QPlan& P, const DepthInfo
 
 // Count of the last depth for the lane's prefix: |∩ rows| minus embedded
 // vertices inside it (rl[j] = index of depth j's vertex in C(u_L) or kInvalid).
-__device__ uint64_t lane_leaf(const QPlan& P, const uint32_t* idx, const uint32_t* rl, uint32_t L) {
+__device__ uint64_t lane_leaf(const QPlan& P, const uint32_t* idx, const uint32_t* rl, uint32_t L, uint32_t& work) {
     const DepthInfo& D = P.dep[L];
     Row drv;
     const uint32_t di = shortest_row(P, D, idx, drv);
+    work += D.nbn == 1 ? 1 : drv.len;
     uint64_t k;
     if (D.nbn == 1) {
         k = drv.len;
@@ -690,9 +817,11 @@ __device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0,
         dp[dd] = 0;
     };
     open(d);
-    uint32_t iter = 0;
+    // work since the last stop test: row elements walked plus leaf counts
+    uint32_t work = 0;
     for (;;) {
-        if ((++iter & 1023u) == 0) {
+        if (++work >= 1024u) {
+            work = 0;
             if (lane_should_stop(A, T.q, T.deadline)) break;
             if (cnt >= (1u << 20)) {
                 const unsigned long long tot = atomicAdd(A.qcount + T.q, cnt) + cnt;
@@ -706,6 +835,7 @@ __device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0,
         while (dp[d] < dl[d]) {
             x = __ldg(de[d] + dp[d]++);
             W.bytes += 4;
+            ++work;
             if (D.nbn > 1 && !in_other_rows(P, D, db[d], idx, x)) continue;
             v = __ldg(D.cand + x);
             W.bytes += 4;
@@ -725,7 +855,7 @@ __device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0,
         rl[d] = rank_in_last(P, v);
         W.nodes++;
         if (d + 1 == L) {
-            cnt += lane_leaf(P, idx, rl, L);
+            cnt += lane_leaf(P, idx, rl, L, work);
             continue;
         }
         ++d;
@@ -775,17 +905,24 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
 #define idx1 slot_idx[1]
 #define vid0 slot_vid[0]
 #define vid1 slot_vid[1]
+    // partials ending at depth 1 (depth 0 is every target's first backward neighbour)
+    if (!compute_parts(P, 1, scr, st, A.gallop_ratio, C, slot_idx)) return;
     uint32_t d = 2;
     LeafState leaf;
     auto open_depth = [&](uint32_t dd) {
-        Row r0, r1;
         const DepthInfo& D = P.dep[dd];
-        const uint32_t k = build_rows<false>(P, D, scr + D.scr_off, st, A.gallop_ratio, C, r0, r1, slot_idx);
-        SLOT_SET(ptr, dd, reinterpret_cast<uint64_t>(r0.p));
-        SLOT_SET(len, dd, k);
+        Row r;
+        if (D.list_off != kInvalid) {
+            r = part_list(scr, D.list_off);
+        } else {
+            const BnRef R = P.bn[D.bn_begin];
+            r = table_row(R, SLOT_GET(idx, R.depth));
+        }
+        SLOT_SET(ptr, dd, reinterpret_cast<uint64_t>(r.p));
+        SLOT_SET(len, dd, r.len);
         SLOT_SET(pos, dd, 0u);
         SLOT_SET(vm, dd, 0u);
-        if (dd + 2 == n && k) leaf_prepare(P, scr, st, A.gallop_ratio, C, slot_idx, slot_vid, leaf);
+        if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf);
     };
     open_depth(2);
     uint32_t iter = 0;
@@ -864,6 +1001,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(idx, d, c);
         SLOT_SET(vid, d, v);
         C.nodes++;
+        if (!compute_parts(P, d, scr, st, A.gallop_ratio, C, slot_idx)) continue;
         ++d;
         open_depth(d);
     }
@@ -1102,7 +1240,10 @@ __device__ void run_cache_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
 }
 
 // ================================================================== kernel
-__global__ void __launch_bounds__(256) enum_kernel(EnumArgs A) {
+// MINB = blocks of 256 threads the register allocation must leave room for
+// on one SM (2: no register cap in practice; 3: at most 80 registers).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
     SMX_EXTERN_SMEM(smem);
     const uint32_t lane = lane_id();
     const uint32_t wib = threadIdx.x >> 5;
@@ -1184,6 +1325,7 @@ struct HostPlanBuild {
     QPlan plan;
     std::vector<BnRef> bn;
     std::vector<OpInfo> op;
+    std::vector<PartRef> part;
     uint64_t scratch_elems = 0;
 };
 
@@ -1228,8 +1370,6 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
         D.bn_begin = (uint32_t)hb.bn.size();
         D.anc = anc[dd];
         D.iter_op = kInvalid;
-        uint32_t cap = 0xffffffffu;       // result <= min over all rows
-        uint32_t cap_other = 0xffffffffu; // the last depth's G leaves out depth n-2's row
         for (uint32_t p : bnd[dd]) {
             BnRef r{};
             r.depth = p;
@@ -1242,24 +1382,60 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                 r.off = T.d_off;
                 r.edge = T.d_edge;
                 r.max_deg = T.max_deg;
-                cap = std::min(cap, T.max_deg);
-                if (p + 2 != n || dd + 1 != n) cap_other = std::min(cap_other, T.max_deg);
             }
             hb.bn.push_back(r);
         }
-        D.scr_off = 0;
-        if (mode == SMX_EXPLORE_CANDIDATES && dd >= 2 && D.nbn >= 2) {
-            D.scr_off = (uint32_t)scr;
-            // result <= min row <= cap; a second cap for the >32-neighbour swap
-            if (dd + 1 == n && cap_other != 0xffffffffu) cap = std::max(cap, cap_other);
-            const uint64_t need = (uint64_t)cap * (D.nbn > 32 ? 2 : 1);
-            scr += (need + 8 + 3) & ~3ull;  // 16-byte aligned buffers
+        D.list_off = kInvalid;
+    }
+    P.leaf_inb = 0;
+    P.leaf_g_bn = P.leaf_g_off = P.leaf_gp_off = kInvalid;
+    if (mode == SMX_EXPLORE_CANDIDATES) {
+        // partial-intersection buffers: word 0 the length, elements from word 4
+        auto alloc = [&](uint64_t cap) {
+            const uint64_t off = scr;
+            scr += (4 + cap + 3) & ~3ull;
+            return (uint32_t)off;
+        };
+        std::vector<std::vector<PartRef>> parts_at(n);
+        for (uint32_t t = 2; t < n; ++t) {
+            DepthInfo& D = P.dep[t];
+            const uint32_t k = D.nbn;
+            const bool leaf = t + 1 == n;
+            const bool inb = leaf && bnd[t][k - 1] + 2 == n;
+            // the last depth's row of depth n-2 is counted per lane, not materialised
+            const uint32_t jmax = inb ? k - 1 : k;
+            uint64_t cap = hb.bn[D.bn_begin].max_deg;
+            uint32_t prev = kInvalid;
+            for (uint32_t j = 2; j <= jmax; ++j) {
+                const uint32_t e = D.bn_begin + j - 1;
+                cap = std::min<uint64_t>(cap, hb.bn[e].max_deg);
+                const uint32_t off = alloc(cap);
+                parts_at[hb.bn[e].depth].push_back(PartRef{D.bn_begin, e, prev, off});
+                prev = off;
+            }
+            if (!leaf) {
+                D.list_off = k >= 2 ? prev : kInvalid;
+            } else {
+                P.leaf_inb = inb ? 1u : 0u;
+                if (jmax >= 2) P.leaf_g_off = prev;
+                else if (jmax == 1) P.leaf_g_bn = D.bn_begin;
+                if (inb && jmax >= 1) P.leaf_gp_off = alloc(cap);
+            }
+        }
+        for (uint32_t dd = 0; dd < n; ++dd) {
+            P.dep[dd].part_begin = (uint32_t)hb.part.size();
+            P.dep[dd].npart = (uint32_t)parts_at[dd].size();
+            hb.part.insert(hb.part.end(), parts_at[dd].begin(), parts_at[dd].end());
         }
     }
     if (mode == SMX_EXPLORE_CANDIDATES) {
         P.ntasks = n >= 2 ? c->tables[c->tab_index[order[0]][order[1]]].e_cnt : 0;
-        // lane depth: the shallowest depth T >= 2 below which (up to n-2) every
-        // candidate list is an intersection of two or more rows, i.e. short
+        // lane depth: given by the caller, or (lane_depth < 0) the shallowest
+        // depth T >= 2 below which (up to n-2) every candidate list is an
+        // intersection of two or more rows.  A lane walks its lists serially,
+        // so this pays only when those intersections stay short; rows of hub
+        // vertices make it far slower than the warp-wide search, hence off
+        // by default.
         uint32_t T = n >= 2 ? n - 2 : 0;
         if (lane_depth < 0) {
             for (uint32_t t = 2; t + 2 < n; ++t) {
@@ -1332,7 +1508,8 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     }
     // device copies of plans; bn / op arrays in one pool
     size_t pool_bytes = 64;
-    for (auto& h : hb) pool_bytes += h.bn.size() * sizeof(BnRef) + h.op.size() * sizeof(OpInfo) + 32;
+    for (auto& h : hb)
+        pool_bytes += h.bn.size() * sizeof(BnRef) + h.op.size() * sizeof(OpInfo) + h.part.size() * sizeof(PartRef) + 48;
     std::vector<char> pool(pool_bytes, 0);
     std::vector<QPlan> plans(nq);
     char* d_pool = nullptr;
@@ -1350,6 +1527,11 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
         if (!hb[i].op.empty()) std::memcpy(pool.data() + at, hb[i].op.data(), hb[i].op.size() * sizeof(OpInfo));
         plans[i].op = reinterpret_cast<const OpInfo*>(d_pool + at);
         at += hb[i].op.size() * sizeof(OpInfo);
+        at = (at + 15) & ~(size_t)15;
+        if (!hb[i].part.empty())
+            std::memcpy(pool.data() + at, hb[i].part.data(), hb[i].part.size() * sizeof(PartRef));
+        plans[i].part = reinterpret_cast<const PartRef*>(d_pool + at);
+        at += hb[i].part.size() * sizeof(PartRef);
     }
     SMX_CUDA_TRY(cudaMemcpyAsync(d_pool, pool.data(), pool_bytes, cudaMemcpyHostToDevice, s));
     SMX_CUDA_TRY(cudaMemcpyAsync(d_plans, plans.data(), nq * sizeof(QPlan), cudaMemcpyHostToDevice, s));
@@ -1360,12 +1542,27 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     const size_t smem = stage_bytes * wpb + 16 * wpb + (size_t)max_ops * sizeof(OpState) * wpb;
     if (smem > 227 * 1024)
         return fail(SMX_TOO_LARGE, "shared memory per block above 227 KB: lower stage_chunk or warps_per_block");
-    SMX_CUDA_TRY(cudaFuncSetAttribute(enum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // blocks_per_sm >= 3 selects the register-capped build of the kernel
+    const bool reg_capped = o.blocks_per_sm >= 3;
+    auto kern = reg_capped ? enum_kernel<3> : enum_kernel<2>;
+    SMX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int bps = 0;
-    SMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, enum_kernel, (int)(wpb * 32), smem));
+    SMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, (int)(wpb * 32), smem));
     if (o.blocks_per_sm > 0) bps = std::min(bps, o.blocks_per_sm);
     if (bps < 1) return fail(SMX_TOO_LARGE, "enumeration kernel does not fit on an SM with this shared-memory size");
-    const uint32_t blocks = (uint32_t)(g->num_sms * bps);
+    uint32_t blocks = (uint32_t)(g->num_sms * bps);
+    {
+        // fewer resident warps when their scratch would not fit in free memory
+        size_t free_b = 0, total_b = 0;
+        SMX_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        const double budget = 0.8 * (double)(free_b + g->scratch_bytes);
+        const double per_block = (double)wpb * (double)scratch_elems * 4.0;
+        if (per_block * blocks > budget) {
+            const uint32_t fit = (uint32_t)(budget / per_block);
+            if (fit < 1) return fail(SMX_TOO_LARGE, "enumeration scratch for one block exceeds device memory");
+            blocks = fit;
+        }
+    }
     const uint64_t nwarps = (uint64_t)blocks * wpb;
     // control block (explicit offsets) + per-warp scratch
     const size_t o_next = 0, o_status = 8, o_stats = 16;           // stats: 5 x u64
@@ -1424,7 +1621,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
         if ((e = cudaMemsetAsync(base, 0, 64, ss)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(d_qcount, 0, nq * 8, ss)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(d_qstop, 0, nq * 4, ss)) != cudaSuccess) return e;
-        SMX_LAUNCH(enum_kernel, blocks, wpb * 32, smem, ss, A);
+        SMX_LAUNCH(kern, blocks, wpb * 32, smem, ss, A);
         return cudaGetLastError();
     };
     cudaGraphExec_t exec = nullptr;

@@ -292,6 +292,7 @@ cudaError_t cudaStreamSynchronize(cudaStream_t s);
 cudaError_t cudaMalloc(void** p, size_t n);
 cudaError_t cudaMallocAsync(void** p, size_t n, cudaStream_t s);
 cudaError_t cudaFree(void* p);
+cudaError_t cudaMemGetInfo(size_t* free_bytes, size_t* total_bytes);
 cudaError_t cudaFreeAsync(void* p, cudaStream_t s);
 cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind k);
 cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind k, cudaStream_t st);

@@ -92,7 +92,7 @@ class Driver:
         o.gallop_ratio = kw.get("gallop_ratio", 4)
         o.task_grab = kw.get("task_grab", 1)
         o.failing_sets = kw.get("failing_sets", 1)
-        o.lane_depth = kw.get("lane_depth", -1)
+        o.lane_depth = kw.get("lane_depth", 0)
         st = _lib.StatsC()
         arr = np.ascontiguousarray(order, dtype=np.uint32)
         rc = self.L.smx_enumerate(g, q, c, p32(arr), ctypes.byref(o), limit, None, ctypes.byref(st))
