@@ -65,7 +65,8 @@ typedef struct {
     int32_t task_grab;        /* tasks a warp takes per queue access; 0 = auto */
     int32_t stage_chunk;      /* elements per warp staged in shared memory for merge intersection */
     int32_t gallop_ratio;     /* long/short length ratio above which binary-search (galloping) intersection is used */
-    int32_t bitmap_min;       /* reserved: list length above which a bitmap probe is used (0 = off) */
+    int32_t bitmap_min;       /* candidate-table mode: |G| (the last depth's list without the row of depth n-2)
+                                 from which G is marked in a bitmap that lanes probe; 0 = auto (32), -1 = never */
     int32_t use_tma;          /* stage rows with cp.async.bulk (1) or plain loads (0) */
     int32_t failing_sets;     /* DAF failing-set pruning in SMX_EXPLORE_CACHE_DAF (1 = on) */
     int32_t lane_depth;       /* candidate-table mode: depth (>= 2) from which each lane enumerates a

@@ -103,6 +103,8 @@ struct QPlan {
     uint32_t leaf_g_bn;    // kInvalid unless G is one row
     uint32_t leaf_g_off;   // kInvalid unless G is a partial buffer
     uint32_t leaf_gp_off;  // buffer for G without the embedded vertices
+    uint32_t leaf_bm;      // 1: G may be marked in the warp's bitmap (indices into C(u_L))
+    uint32_t pad2;
     DepthInfo dep[kMaxQ];
 };
 
@@ -118,7 +120,10 @@ struct EnumArgs {
     int* status;                    // 0 ok, SMX_TIMEOUT, SMX_STOPPED, SMX_CUDA_ERROR
     const volatile uint32_t* host_stop;
     uint64_t scratch_stride;        // elements per warp
+    uint32_t* bitmap;               // per warp membership bitmap of the last depth's G (or null)
+    uint64_t bm_stride;             // bitmap words per warp
     uint64_t budget_ns;             // time budget per warp from its start, 0 = none
+    uint32_t bitmap_min;            // |G| from which the bitmap is used
     uint32_t nq;
     uint32_t max_ops;               // op-state entries per warp (cache mode)
     uint32_t grab;
@@ -126,7 +131,6 @@ struct EnumArgs {
     uint32_t gallop_ratio;
     uint32_t use_tma;
     uint32_t failing_sets;
-    uint32_t pad;
 };
 
 // ------------------------------------------------------------------ staging
@@ -547,10 +551,39 @@ struct LeafState {
     BnRef row;         // E[u_{n-2}][u_L] when inb
     uint32_t prank0, prank1;
     uint64_t pmask;    // depths with a valid prank
+    uint32_t* bm;      // the warp bitmap while G is marked in it, else null
 };
 
+// Per-lane |row ∩ G| by probing G's membership bitmap: one independent load
+// per row element (L2, where the warp's atomics set the bits).
+__device__ __forceinline__ uint32_t lane_count_bitmap(const uint32_t* row, uint32_t n, const uint32_t* bm) {
+    uint32_t cnt = 0, i = 0;
+    for (; i + 4 <= n; i += 4) {
+        const uint32_t x0 = __ldg(row + i), x1 = __ldg(row + i + 1), x2 = __ldg(row + i + 2), x3 = __ldg(row + i + 3);
+        const uint32_t w0 = __ldcg(bm + (x0 >> 5)), w1 = __ldcg(bm + (x1 >> 5));
+        const uint32_t w2 = __ldcg(bm + (x2 >> 5)), w3 = __ldcg(bm + (x3 >> 5));
+        cnt += ((w0 >> (x0 & 31)) & 1u) + ((w1 >> (x1 & 31)) & 1u) + ((w2 >> (x2 & 31)) & 1u) + ((w3 >> (x3 & 31)) & 1u);
+    }
+    for (; i < n; ++i) {
+        const uint32_t x = __ldg(row + i);
+        cnt += (__ldcg(bm + (x >> 5)) >> (x & 31)) & 1u;
+    }
+    return cnt;
+}
+
+// Unmarks G in the warp bitmap (G is still where leaf_prepare put it: nothing
+// else runs at depth n-2).
+__device__ void leaf_clear(LeafState& S) {
+    if (!S.bm) return;
+    const uint32_t* g = reinterpret_cast<const uint32_t*>(S.gptr);
+    __syncwarp();
+    for (uint32_t i = lane_id(); i < S.glen; i += 32) atomicAnd(S.bm + (g[i] >> 5), ~(1u << (g[i] & 31)));
+    __syncwarp();
+    S.bm = nullptr;
+}
+
 __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uint32_t (&slot_idx)[2],
-                             const uint32_t (&slot_vid)[2], LeafState& S) {
+                             const uint32_t (&slot_vid)[2], LeafState& S, uint32_t* bm, uint32_t bitmap_min) {
     const uint32_t lane = lane_id();
     const uint32_t L = P.n - 1;
     const DepthInfo& D = P.dep[L];
@@ -620,6 +653,11 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uin
         S.glen = k;
         S.pmask = 0;
         S.k0 = k;
+        if (bm && P.leaf_bm && k >= bitmap_min) {
+            for (uint32_t i = lane; i < k; i += 32) atomicOr(bm + (dst[i] >> 5), 1u << (dst[i] & 31));
+            __syncwarp();
+            S.bm = bm;
+        }
     }
 }
 
@@ -649,8 +687,16 @@ __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_
             const Row r = table_row(S.row, c);
             row = r.p;
             row_len = r.len;
-            cnt = S.gany ? lane_count_common(r.p, r.len, reinterpret_cast<const uint32_t*>(S.gptr), S.glen) : r.len;
-            bytes = 12 + (S.gany ? 4 * (r.len + S.glen) : 0);
+            if (S.bm && r.len <= S.glen * (32u - __clz(r.len))) {
+                // probes of the bitmap (independent loads) cost less than
+                // |G| searches of the row (dependent loads)
+                cnt = lane_count_bitmap(r.p, r.len, S.bm);
+                bytes = 12 + 8 * r.len;
+            } else {
+                cnt = S.gany ? lane_count_common(r.p, r.len, reinterpret_cast<const uint32_t*>(S.gptr), S.glen)
+                             : r.len;
+                bytes = 12 + (S.gany ? 4 * (r.len + S.glen) : 0);
+            }
         }
     }
     if (S.inb && S.pmask) {
@@ -865,8 +911,8 @@ __device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0,
 }
 
 // One task: root r = row of entry t in E[o0][o1], depth-1 candidate edge[t].
-__device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, Stage& st, Counters& C,
-                               Tally& T) {
+__device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, uint32_t* bm, Stage& st,
+                               Counters& C, Tally& T) {
     unsigned long long& local = T.local;
     const uint32_t lane = lane_id();
     const uint32_t n = P.n;
@@ -909,6 +955,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
     if (!compute_parts(P, 1, scr, st, A.gallop_ratio, C, slot_idx)) return;
     uint32_t d = 2;
     LeafState leaf;
+    leaf.bm = nullptr;
     auto open_depth = [&](uint32_t dd) {
         const DepthInfo& D = P.dep[dd];
         Row r;
@@ -922,7 +969,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(len, dd, r.len);
         SLOT_SET(pos, dd, 0u);
         SLOT_SET(vm, dd, 0u);
-        if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf);
+        if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf, bm, A.bitmap_min);
     };
     open_depth(2);
     uint32_t iter = 0;
@@ -933,6 +980,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
             const uint32_t pos = SLOT_GET(pos, d);
             const uint32_t len = SLOT_GET(len, d);
             if (pos >= len) {
+                if (d + 2 == n) leaf_clear(leaf);
                 if (d == 2) break;
                 --d;
                 continue;
@@ -1005,6 +1053,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         ++d;
         open_depth(d);
     }
+    leaf_clear(leaf);  // a stop can leave depth n-2 early
 #undef idx0
 #undef idx1
 #undef vid0
@@ -1269,6 +1318,12 @@ __global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
 #endif
     __syncwarp();
     uint32_t* scr = A.scratch + (size_t)gw * A.scratch_stride;
+    // the bitmap starts empty; every task leaves it empty again
+    uint32_t* bm = A.bitmap ? A.bitmap + (size_t)gw * A.bm_stride : nullptr;
+    if (bm) {
+        for (uint64_t i = lane; i < A.bm_stride; i += 32) bm[i] = 0;
+        __syncwarp();
+    }
     const uint64_t deadline = A.budget_ns ? global_timer_ns() + A.budget_ns : 0;
     Counters C;
     Tally T;
@@ -1300,7 +1355,7 @@ __global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
             const QPlan& P = A.plans[q];
             T.q = q;
             T.local = 0;
-            if (P.mode == SMX_EXPLORE_CANDIDATES) run_table_task(A, P, t - qlo, scr, st, C, T);
+            if (P.mode == SMX_EXPLORE_CANDIDATES) run_table_task(A, P, t - qlo, scr, bm, st, C, T);
             else run_cache_task(A, P, t - qlo, scr, wops, st, C, T);
             flush_tally(A, T);
             if (st.failed) break;
@@ -1327,10 +1382,11 @@ struct HostPlanBuild {
     std::vector<OpInfo> op;
     std::vector<PartRef> part;
     uint64_t scratch_elems = 0;
+    uint64_t bm_words = 0;  // last-depth bitmap words per warp (0: none)
 };
 
 int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order, int mode,
-                    int lane_depth, HostPlanBuild& hb) {
+                    int lane_depth, bool use_bitmap, HostPlanBuild& hb) {
     const uint32_t n = q.n;
     std::memset(&hb.plan, 0, sizeof(QPlan));
     QPlan& P = hb.plan;
@@ -1388,6 +1444,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
         D.list_off = kInvalid;
     }
     P.leaf_inb = 0;
+    P.leaf_bm = 0;
     P.leaf_g_bn = P.leaf_g_off = P.leaf_gp_off = kInvalid;
     if (mode == SMX_EXPLORE_CANDIDATES) {
         // partial-intersection buffers: word 0 the length, elements from word 4
@@ -1419,7 +1476,13 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                 P.leaf_inb = inb ? 1u : 0u;
                 if (jmax >= 2) P.leaf_g_off = prev;
                 else if (jmax == 1) P.leaf_g_bn = D.bn_begin;
-                if (inb && jmax >= 1) P.leaf_gp_off = alloc(cap);
+                if (inb && jmax >= 1) {
+                    P.leaf_gp_off = alloc(cap);
+                    if (use_bitmap) {
+                        P.leaf_bm = 1;
+                        hb.bm_words = (uint64_t)c->cnt[order[t]] / 32 + 1;
+                    }
+                }
             }
         }
         for (uint32_t dd = 0; dd < n; ++dd) {
@@ -1498,11 +1561,13 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     std::vector<HostPlanBuild> hb(nq);
     std::vector<uint64_t> prefix(nq + 1, 0);
     uint64_t scratch_elems = 8;
+    uint64_t bm_words = 0;
     uint32_t max_ops = 1;
     for (uint32_t i = 0; i < nq; ++i) {
-        int rc = build_host_plan(g, *qs[i], cs[i], orders[i], mode, o.lane_depth, hb[i]);
+        int rc = build_host_plan(g, *qs[i], cs[i], orders[i], mode, o.lane_depth, o.bitmap_min >= 0, hb[i]);
         if (rc != SMX_OK) return rc;
         scratch_elems = std::max(scratch_elems, hb[i].scratch_elems);
+        bm_words = std::max(bm_words, hb[i].bm_words);
         max_ops = std::max(max_ops, hb[i].plan.nops);
         prefix[i + 1] = prefix[i] + hb[i].plan.ntasks;
     }
@@ -1556,7 +1621,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
         size_t free_b = 0, total_b = 0;
         SMX_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         const double budget = 0.8 * (double)(free_b + g->scratch_bytes);
-        const double per_block = (double)wpb * (double)scratch_elems * 4.0;
+        const double per_block = (double)wpb * (double)(scratch_elems + bm_words) * 4.0;
         if (per_block * blocks > budget) {
             const uint32_t fit = (uint32_t)(budget / per_block);
             if (fit < 1) return fail(SMX_TOO_LARGE, "enumeration scratch for one block exceeds device memory");
@@ -1571,7 +1636,8 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     const size_t o_prefix = o_qlimit + (size_t)nq * 8;
     const size_t o_qstop = o_prefix + (size_t)(nq + 1) * 8;
     const size_t o_scr = (o_qstop + (size_t)nq * 4 + 255) & ~(size_t)255;
-    const size_t total_bytes = o_scr + nwarps * scratch_elems * 4 + 64;
+    const size_t o_bm = (o_scr + nwarps * scratch_elems * 4 + 255) & ~(size_t)255;
+    const size_t total_bytes = o_bm + nwarps * bm_words * 4 + 64;
     int rc = ensure_scratch(g, total_bytes);
     if (rc != SMX_OK) return rc;
     char* base = static_cast<char*>(g->d_scratch);
@@ -1605,6 +1671,9 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     A.status = d_status;
     A.host_stop = d_host_stop;
     A.scratch_stride = scratch_elems;
+    A.bitmap = bm_words ? reinterpret_cast<uint32_t*>(base + o_bm) : nullptr;
+    A.bm_stride = bm_words;
+    A.bitmap_min = o.bitmap_min > 0 ? (uint32_t)o.bitmap_min : 32u;
     A.budget_ns = o.time_budget_ms > 0 ? (uint64_t)(o.time_budget_ms * 1e6) : 0;
     A.nq = nq;
     A.max_ops = max_ops;

@@ -3,10 +3,13 @@
 // TEST INFRASTRUCTURE ONLY.  tests/emu/Makefile compiles the product sources
 // (subgraphmatching_b200/csrc/*.cu, *.cpp) with g++ -DSMX_EMU against this
 // header into tests/emu/libsmx_emu.so, so the kernels' warp-level logic can be
-// checked against the oracle on machines without a GPU.  Every warp runs as 32
-// host threads; shuffles, ballots and reductions meet at a per-warp barrier;
-// __syncthreads at a per-block barrier.  "Device" memory is host memory.  The
-// product package never loads this library.
+// checked against the oracle on machines without a GPU.  Every GPU thread runs
+// as a fiber (its own stack, switched cooperatively on one host thread; with
+// -DEMU_THREADS as a host thread instead, which AddressSanitizer builds use);
+// shuffles, ballots and reductions meet at a per-warp barrier, __syncthreads
+// at a per-block barrier, and a fiber waiting at a barrier yields to the
+// others.  "Device" memory is host memory.  The product package never loads
+// this library.
 #pragma once
 
 #include <algorithm>
@@ -49,9 +52,40 @@ struct uint2 {
 
 namespace emu {
 
+#ifdef EMU_THREADS
+using Bar = std::barrier<>;
+#else
+void fiber_yield();
+// Barrier among the fibers of one host thread: waiting fibers yield until the
+// last arrival opens the next generation.
+struct Bar {
+    explicit Bar(unsigned n) : expected(n) {}
+    unsigned expected;
+    unsigned count = 0;
+    uint64_t gen = 0;
+    void arrive_and_wait() {
+        const uint64_t g = gen;
+        if (++count >= expected) {
+            count = 0;
+            ++gen;
+            return;
+        }
+        while (gen == g) fiber_yield();
+    }
+    void arrive_and_drop() {
+        --expected;
+        if (expected > 0 && count >= expected) {
+            count = 0;
+            ++gen;
+        }
+    }
+};
+void run_fibers(unsigned n, const std::function<void(unsigned)>& body);
+#endif
+
 struct Block {
-    std::unique_ptr<std::barrier<>> bar;
-    std::vector<std::unique_ptr<std::barrier<>>> warp_bar;
+    std::unique_ptr<Bar> bar;
+    std::vector<std::unique_ptr<Bar>> warp_bar;
     std::vector<std::vector<uint64_t>> warp_slot;
     std::vector<unsigned char> dyn;
     std::mutex mu;
@@ -107,31 +141,34 @@ void launch_now(void (*k)(P...), dim3 grid, dim3 block, size_t smem, std::tuple<
     for (unsigned by = 0; by < grid.y; ++by)
         for (unsigned bx = 0; bx < grid.x; ++bx) {
             Block B;
-            B.bar = std::make_unique<std::barrier<>>(nthreads);
+            B.bar = std::make_unique<Bar>(nthreads);
             const unsigned nw = nthreads / 32;
             for (unsigned w = 0; w < nw; ++w) {
-                B.warp_bar.push_back(std::make_unique<std::barrier<>>(32));
+                B.warp_bar.push_back(std::make_unique<Bar>(32));
                 B.warp_slot.emplace_back(32, 0);
             }
             B.dyn.assign(smem + 64, 0);
+            auto body = [&](unsigned t) {
+                ctx.tid = dim3(t, 0, 0);
+                ctx.bid = dim3(bx, by, 0);
+                ctx.bdim = block;
+                ctx.gdim = grid;
+                ctx.blk = &B;
+                ctx.warp = t / 32;
+                ctx.lane = t % 32;
+                std::tuple<std::decay_t<P>...> mine = params;
+                std::apply(k, mine);
+                B.warp_bar[ctx.warp]->arrive_and_drop();
+                B.bar->arrive_and_drop();
+            };
+#ifdef EMU_THREADS
             std::vector<std::thread> th;
             th.reserve(nthreads);
-            for (unsigned t = 0; t < nthreads; ++t) {
-                th.emplace_back([&, t]() {
-                    ctx.tid = dim3(t, 0, 0);
-                    ctx.bid = dim3(bx, by, 0);
-                    ctx.bdim = block;
-                    ctx.gdim = grid;
-                    ctx.blk = &B;
-                    ctx.warp = t / 32;
-                    ctx.lane = t % 32;
-                    std::tuple<std::decay_t<P>...> mine = params;
-                    std::apply(k, mine);
-                    B.warp_bar[ctx.warp]->arrive_and_drop();
-                    B.bar->arrive_and_drop();
-                });
-            }
+            for (unsigned t = 0; t < nthreads; ++t) th.emplace_back(body, t);
             for (auto& x : th) x.join();
+#else
+            run_fibers(nthreads, body);
+#endif
         }
 }
 
@@ -252,6 +289,10 @@ inline int atomicCAS(int* p, int cmp, int v) {
     return cmp;
 }
 inline unsigned atomicExch(unsigned* p, unsigned v) { return __atomic_exchange_n(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicAnd(unsigned* p, unsigned v) { return __atomic_fetch_and(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicOr(unsigned* p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned __ldcg(const unsigned* p) { return __atomic_load_n(p, __ATOMIC_SEQ_CST); }
+inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }
 inline unsigned long long atomicAnd(unsigned long long* p, unsigned long long v) {
     return __atomic_fetch_and(p, v, __ATOMIC_SEQ_CST);
 }

@@ -4,6 +4,102 @@
 namespace emu {
 thread_local Ctx ctx;
 
+#ifndef EMU_THREADS
+// ------------------------------------------------------------------ fibers
+// x86-64 System V context switch: saves the callee-saved registers and the
+// stack pointer of the running context into *save, resumes the one at `to`.
+extern "C" void emu_fiber_switch(void** save, void* to);
+asm(R"(
+    .text
+    .globl emu_fiber_switch
+    .type emu_fiber_switch,@function
+emu_fiber_switch:
+    pushq %rbp
+    pushq %rbx
+    pushq %r12
+    pushq %r13
+    pushq %r14
+    pushq %r15
+    movq %rsp, (%rdi)
+    movq %rsi, %rsp
+    popq %r15
+    popq %r14
+    popq %r13
+    popq %r12
+    popq %rbx
+    popq %rbp
+    ret
+    .size emu_fiber_switch,.-emu_fiber_switch
+)");
+
+namespace {
+constexpr size_t kFiberStack = 256 * 1024;
+struct Fiber {
+    void* sp = nullptr;
+    Ctx ctx;
+    bool done = false;
+};
+struct Sched {
+    void* main_sp = nullptr;
+    std::vector<Fiber> fibers;
+    size_t cur = 0;
+    const std::function<void(unsigned)>* body = nullptr;
+};
+thread_local Sched* g_sched = nullptr;
+}  // namespace
+
+extern "C" void emu_fiber_entry() {
+    Sched* S = g_sched;
+    const size_t me = S->cur;
+    (*S->body)((unsigned)me);
+    S->fibers[me].done = true;
+    S->fibers[me].ctx = ctx;
+    emu_fiber_switch(&S->fibers[me].sp, S->main_sp);
+    std::abort();  // a finished fiber is never resumed
+}
+
+void fiber_yield() {
+    Sched* S = g_sched;
+    Fiber& f = S->fibers[S->cur];
+    f.ctx = ctx;
+    emu_fiber_switch(&f.sp, S->main_sp);
+    ctx = S->fibers[S->cur].ctx;
+}
+
+void run_fibers(unsigned n, const std::function<void(unsigned)>& body) {
+    Sched S;
+    S.body = &body;
+    S.fibers.resize(n);
+    std::vector<char*> stacks(n);
+    for (unsigned i = 0; i < n; ++i) {
+        stacks[i] = static_cast<char*>(std::malloc(kFiberStack));
+        if (!stacks[i]) std::abort();
+        uintptr_t top = (reinterpret_cast<uintptr_t>(stacks[i]) + kFiberStack) & ~(uintptr_t)15;
+        void** sp = reinterpret_cast<void**>(top);
+        *--sp = nullptr;                                         // alignment pad
+        *--sp = reinterpret_cast<void*>(&emu_fiber_entry);       // popped by ret
+        for (int r = 0; r < 6; ++r) *--sp = nullptr;             // rbp rbx r12-r15
+        S.fibers[i].sp = sp;
+    }
+    Sched* saved = g_sched;
+    const Ctx saved_ctx = ctx;
+    g_sched = &S;
+    unsigned alive = n;
+    while (alive) {
+        for (unsigned i = 0; i < n; ++i) {
+            if (S.fibers[i].done) continue;
+            S.cur = i;
+            ctx = S.fibers[i].ctx;
+            emu_fiber_switch(&S.main_sp, S.fibers[i].sp);
+            if (S.fibers[i].done) --alive;
+        }
+    }
+    g_sched = saved;
+    ctx = saved_ctx;
+    for (char* p : stacks) std::free(p);
+}
+#endif
+
 Capture& capture() {
     static thread_local Capture c;
     return c;

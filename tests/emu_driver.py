@@ -93,6 +93,7 @@ class Driver:
         o.task_grab = kw.get("task_grab", 1)
         o.failing_sets = kw.get("failing_sets", 1)
         o.lane_depth = kw.get("lane_depth", 0)
+        o.bitmap_min = kw.get("bitmap_min", 0)
         st = _lib.StatsC()
         arr = np.ascontiguousarray(order, dtype=np.uint32)
         rc = self.L.smx_enumerate(g, q, c, p32(arr), ctypes.byref(o), limit, None, ctypes.byref(st))

@@ -84,8 +84,9 @@ def test_emulated_limit_and_batch(emu, port):
 
 def test_emulated_lane_subtrees_and_galloping(emu, port):
     """Per-lane subtree enumeration below the lane depth (chosen from the
-    query, or forced to depth 2) and the galloping intersection (ratio 1, so
-    every long row is probed by binary search) give the oracle's counts."""
+    query, or forced to depth 2), the galloping intersection (ratio 1, so
+    every long row is probed by binary search) and the last-depth bitmap give
+    the oracle's counts."""
     g, gpath = host_graph(900, 4000, 2.2, 1, 5)
     off, nb, lab = g.csr()
     dg = emu.graph(off, nb, lab)
@@ -103,4 +104,6 @@ def test_emulated_lane_subtrees_and_galloping(emu, port):
         for lane_depth in (-1, 2):
             assert emu.enumerate(dg, dq, c, order, explore=0, lane_depth=lane_depth).count == ref
         assert emu.enumerate(dg, dq, c, order, explore=0, lane_depth=0, gallop_ratio=1).count == ref
+        for bmin in (1, -1):  # last depth through the bitmap from one element / never
+            assert emu.enumerate(dg, dq, c, order, explore=0, bitmap_min=bmin).count == ref
         assert emu.enumerate(dg, dq, c, order, explore=1, gallop_ratio=1).count == ref

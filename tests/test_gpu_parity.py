@@ -139,6 +139,25 @@ def test_lane_depths_agree(gpu, golden):
                     assert st.count == qc["count"], (gcase["name"], qc["k"], qc["seed"], ld, ratio, st.count)
 
 
+def test_leaf_bitmap_agrees(gpu, golden):
+    """Last-depth counts through the membership bitmap (forced on from one
+    element, default threshold, off) give the golden counts."""
+    for gcase in golden["graphs"]:
+        hg, dg, _ = device_graph(gcase["n"], gcase["m"], gcase["gamma"], gcase["labels"], gcase["seed"])
+        for qc in gcase["queries"]:
+            if qc["k"] < 4 or (qc["cap"] == 0 and qc["count"] > BIG):
+                continue
+            q, _ = query_file(hg, qc["k"], qc["dense"], qc["seed"])
+            can = smx.CandidateParam(dg, q)
+            if not smx.Filter_GQL(dg, q, can):
+                continue
+            for bmin in (1, 0, -1):
+                opts = smx.EnumOptions(explore=smx.EXPLORE_CANDIDATES, bitmap_min=bmin)
+                st = smx.explore(dg, q, can, qc["order_ri"], opts, qc["cap"])
+                assert st.status == 0
+                assert st.count == qc["count"], (gcase["name"], qc["k"], qc["seed"], bmin, st.count)
+
+
 def test_edge_cases(gpu):
     hg, dg, _ = device_graph(2000, 9000, 2.5, 4, 3)
     _, _, lab = hg.csr()
