@@ -191,6 +191,10 @@ void smx_graph_destroy(smx_graph* g) {
     }
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
+    for (smx_cand* c : g->cands) {  // candidate sets still alive lose their device memory
+        free_cand_device(c);
+        c->g = nullptr;
+    }
     cudaFree(g->d_off);
     cudaFree(g->d_adj);
     cudaFree(g->d_lab);
@@ -323,6 +327,7 @@ int smx_order_ri(const smx_query* q, uint32_t* order) {
 int smx_order_gql(const smx_query* q, const smx_cand* c, uint32_t* order) {
     if (!q || !c || !order) return fail(SMX_BAD_ARGUMENT, "null argument");
     if (c->qn != q->h.n) return fail(SMX_BAD_ARGUMENT, "candidates belong to another query");
+    if (!c->g) return fail(SMX_BAD_ARGUMENT, "the candidate set's data graph was destroyed");
     order_gql(q->h, c->cnt.data(), c->g->h.n, order);
     return SMX_OK;
 }
@@ -347,6 +352,7 @@ int smx_filter(smx_graph* g, const smx_query* q, int kind, int build_tables, smx
         return rc;
     }
     if (rc == SMX_EMPTY_CANDIDATES) set_error("a query vertex has no candidates");
+    g->cands.push_back(c);
     *out = c;
     return rc;
 }
@@ -360,6 +366,7 @@ int smx_cand_counts(const smx_cand* c, uint32_t* counts) {
 int smx_cand_export(const smx_cand* c, uint32_t u, uint32_t* out) {
     if (!c || !out) return fail(SMX_BAD_ARGUMENT, "null argument");
     if (u >= c->qn) return fail(SMX_BAD_ARGUMENT, "query vertex out of range");
+    if (!c->g) return fail(SMX_BAD_ARGUMENT, "the candidate set's data graph was destroyed");
     if (u >= c->cnt.size() || c->cnt[u] == 0 || !c->d_cand) return SMX_OK;
     cudaSetDevice(c->g->device);
     SMX_CUDA_TRY(cudaMemcpy(out, c->cand_ptr(u), c->cnt[u] * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -368,6 +375,7 @@ int smx_cand_export(const smx_cand* c, uint32_t u, uint32_t* out) {
 
 int smx_table_info(const smx_cand* c, uint32_t a, uint32_t b, uint32_t* v_cnt, uint32_t* e_cnt, uint32_t* max_degree) {
     if (!c) return fail(SMX_BAD_ARGUMENT, "null argument");
+    if (!c->g) return fail(SMX_BAD_ARGUMENT, "the candidate set's data graph was destroyed");
     if (a >= c->qn || b >= c->qn || c->tab_index[a][b] < 0) return fail(SMX_BAD_ARGUMENT, "no table for this pair");
     const DevTable& t = c->tables[c->tab_index[a][b]];
     if (v_cnt) *v_cnt = t.v_cnt;
@@ -379,6 +387,7 @@ int smx_table_info(const smx_cand* c, uint32_t a, uint32_t b, uint32_t* v_cnt, u
 int smx_table_export(const smx_cand* c, uint32_t a, uint32_t b, uint32_t* offsets, uint32_t* edge, uint32_t* edge_v) {
     if (!c) return fail(SMX_BAD_ARGUMENT, "null argument");
     if (a >= c->qn || b >= c->qn || c->tab_index[a][b] < 0) return fail(SMX_BAD_ARGUMENT, "no table for this pair");
+    if (!c->g) return fail(SMX_BAD_ARGUMENT, "the candidate set's data graph was destroyed");
     const DevTable& t = c->tables[c->tab_index[a][b]];
     cudaSetDevice(c->g->device);
     if (offsets) SMX_CUDA_TRY(cudaMemcpy(offsets, t.d_off, (t.v_cnt + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -401,6 +410,10 @@ int smx_cand_timing(const smx_cand* c, double* ms4) {
 
 void smx_cand_destroy(smx_cand* c) {
     if (!c) return;
+    if (c->g) {
+        auto& v = c->g->cands;
+        v.erase(std::remove(v.begin(), v.end(), c), v.end());
+    }
     free_cand_device(c);
     delete c;
 }

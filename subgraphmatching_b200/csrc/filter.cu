@@ -616,7 +616,7 @@ int upload_graph(smx_graph* g) {
 }
 
 void free_cand_device(smx_cand* c) {
-    if (!c || !c->g) return;
+    if (!c || !c->g) return;  // no graph: freed when the graph was destroyed
     cudaSetDevice(c->g->device);
     cudaStream_t st = c->g->stream;
     if (c->d_mask) cudaFreeAsync(c->d_mask, st);

@@ -105,7 +105,12 @@ struct smx_graph {
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
     cudaEvent_t mark[2] = {nullptr, nullptr};
+    // candidate sets built on this graph: destroying the graph frees their
+    // device memory and detaches them (their handles stay valid to destroy)
+    std::vector<smx_cand*> cands;
 };
+
+struct smx_cand;
 
 struct smx_query {
     smx::HostQuery h;
@@ -113,7 +118,7 @@ struct smx_query {
 };
 
 struct smx_cand {
-    smx_graph* g = nullptr;
+    smx_graph* g = nullptr;  // null once the graph was destroyed
     uint32_t qn = 0;
     int kind = 0;
     int ok = 0;

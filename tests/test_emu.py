@@ -8,6 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from emu_driver import p32
 from helpers import host_graph, query_file
 
 CASES = [  # (n, m, labels, seed, [(k, dense, qseed)], filter kinds)
@@ -107,3 +108,23 @@ def test_emulated_lane_subtrees_and_galloping(emu, port):
         for bmin in (1, -1):  # last depth through the bitmap from one element / never
             assert emu.enumerate(dg, dq, c, order, explore=0, bitmap_min=bmin).count == ref
         assert emu.enumerate(dg, dq, c, order, explore=1, gallop_ratio=1).count == ref
+
+
+def test_emulated_graph_destroyed_before_its_candidates(emu):
+    """Finalizers may run in any order (Python's cycle collector): a data graph
+    destroyed before a candidate set built on it frees that set's device
+    memory and detaches it; the set's handle then refuses device reads with
+    SMX_BAD_ARGUMENT and can still be destroyed."""
+    g, _ = host_graph(300, 900, 2.5, 1, 5)
+    off, nb, lab = g.csr()
+    dg = emu.graph(off, nb, lab)
+    q, _ = query_file(g, 4, True, 2)
+    qo, qn, ql = q.csr()
+    dq = emu.query(qo, qn, ql)
+    c, ok = emu.filter(dg, dq, 1)
+    assert ok
+    emu.L.smx_graph_destroy(dg)
+    assert emu.table(c, 0, 1) is None
+    assert emu.L.smx_cand_export(c, 0, p32(np.zeros(8, dtype=np.uint32))) == 6  # SMX_BAD_ARGUMENT
+    emu.L.smx_cand_destroy(c)
+    emu.L.smx_query_destroy(dq)
