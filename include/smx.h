@@ -189,6 +189,34 @@ int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand
                         const uint32_t* const* orders, uint32_t nq, const smx_enum_opts* opts,
                         uint64_t limit, uint64_t* counts, smx_stats* out);
 
+/* ------------------------------------------------------------ enumeration without allocation */
+/* No counterpart in the reference.  smx_enumerate allocates device memory on
+ * every call (its plans, and scratch that grows with the query); some callers
+ * cannot allow that -- a framework whose own caching allocator has already
+ * reserved the GPU's memory, code that must not pay cudaMalloc's implicit
+ * device synchronisation or risk its failure mid-run, or a service that has
+ * to keep a fixed device footprint after start-up.  smx_enumerate_noalloc
+ * counts like smx_enumerate (same arguments, same counts and statistics;
+ * kernel_ms is host-timed) but calls no cudaMalloc/cudaFree or other
+ * allocating routine: its control block, plan and per-warp scratch live in
+ * one static device array of SMX_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * this library reserves until the process exits.  The caller still passes the
+ * graph, query and candidate handles (made by the allocating calls above) and
+ * receives the result in *out.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture on the graph's stream.
+ *  - Every call shares the array, which keeps the last call's contents; each
+ *    call clears what must start at zero.  Two calls whose GPU work overlapped
+ *    would race on it, so calls are serialised by a process-wide lock and each
+ *    waits for its own launch before returning.
+ *  - It launches only as many warps as the array holds; a query whose one
+ *    block of warps_per_block warps needs more than the array returns
+ *    SMX_TOO_LARGE with the sizes in smx_last_error(). */
+#define SMX_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int smx_enumerate_noalloc(smx_graph* g, const smx_query* q, const smx_cand* c, const uint32_t* order,
+                          const smx_enum_opts* opts, uint64_t limit, volatile uint32_t* stop, smx_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,8 @@ SIGNATURES = [
     ("smx_cand_destroy", None, [_vp]),
     ("smx_enum_opts_default", None, [ctypes.POINTER(EnumOpts)]),
     ("smx_enumerate", _i32, [_vp, _vp, _vp, _pu32, ctypes.POINTER(EnumOpts), _u64, _pu32, ctypes.POINTER(StatsC)]),
+    ("smx_enumerate_noalloc", _i32, [_vp, _vp, _vp, _pu32, ctypes.POINTER(EnumOpts), _u64, _pu32,
+                                     ctypes.POINTER(StatsC)]),
     ("smx_stop_flag_create", _i32, [_i32, ctypes.POINTER(_pu32)]),
     ("smx_stop_flag_destroy", None, [_pu32]),
     ("smx_enumerate_batch", _i32, [_vp, _pvp, _pvp, ctypes.POINTER(_pu32), _u32, ctypes.POINTER(EnumOpts), _u64,

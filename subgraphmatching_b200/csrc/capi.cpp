@@ -467,6 +467,32 @@ int smx_enumerate(smx_graph* g, const smx_query* q, const smx_cand* c, const uin
     return device_enumerate(g, qs, cs, os, o, lim, stop, &count, out, false);
 }
 
+int smx_enumerate_noalloc(smx_graph* g, const smx_query* q, const smx_cand* c, const uint32_t* order,
+                          const smx_enum_opts* opts, uint64_t limit, volatile uint32_t* stop, smx_stats* out) {
+    if (!g || !q || !c) return fail(SMX_BAD_ARGUMENT, "null argument");
+    if (c->qn != q->h.n || c->g != g) return fail(SMX_BAD_ARGUMENT, "candidates belong to another query or graph");
+    if (out) std::memset(out, 0, sizeof(*out));
+    if (!c->ok) return fail(SMX_EMPTY_CANDIDATES, "candidate sets are empty");
+    smx_enum_opts o;
+    if (opts) o = *opts; else smx_enum_opts_default(&o);
+    if (o.explore != SMX_EXPLORE_CANDIDATES && o.explore != SMX_EXPLORE_CACHE_DAF)
+        return fail(SMX_BAD_ARGUMENT, "unknown explore kind");
+    std::vector<uint32_t> ord(q->h.n);
+    if (order) std::copy(order, order + q->h.n, ord.begin());
+    else order_ri(q->h, ord.data());
+    if (!order_valid(q->h, ord.data())) return fail(SMX_INVALID_ORDER, "order is not a connected permutation of the query vertices");
+    if (q->h.n == 1) {
+        const uint64_t raw = c->cnt[ord[0]];
+        if (out) {
+            out->count = limit && raw > limit ? limit : raw;
+            out->raw_count = raw;
+            out->limit_reached = limit && raw >= limit;
+        }
+        return SMX_OK;
+    }
+    return device_enumerate_noalloc(g, q->h, c, ord.data(), o, limit, stop, out);
+}
+
 int smx_stop_flag_create(int device, volatile uint32_t** flag) {
     if (!flag) return fail(SMX_BAD_ARGUMENT, "null argument");
     *flag = nullptr;

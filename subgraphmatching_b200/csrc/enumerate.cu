@@ -27,7 +27,9 @@
 // The last depth is never materialised: its count is |intersection| minus the
 // already-embedded vertices that fall in it (rank lookups + membership tests).
 #include <algorithm>
+#include <chrono>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1765,6 +1767,172 @@ int ensure_scratch(smx_graph* g, size_t bytes) {
     SMX_CUDA_TRY(cudaMalloc(&g->d_scratch, bytes));
     g->scratch_bytes = bytes;
     return SMX_OK;
+}
+
+// ------------------------------------------------------------------ enumeration without allocation
+// smx_enumerate allocates device memory on every call (plans, and scratch
+// that grows with the query).  Some callers cannot allow that: a host
+// framework whose own caching allocator has reserved the device memory, code
+// that must not take cudaMalloc's implicit device synchronisation or its
+// failure when memory is exhausted, or a process that has to keep its device
+// footprint fixed after start-up.  For them smx_enumerate_noalloc runs the
+// same kernel with all of its working memory (control block, plans, per-warp
+// scratch and bitmaps) in the file-scope array below, reserved when the
+// library is loaded on a GPU and held until the process exits.  The array is
+// shared by every call on that device and keeps the last call's contents; the
+// parts that must start at zero are cleared by each call.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SMX_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;                       // calls never overlap on the GPU
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address of the array, per device
+
+// Once per device, with that device current: the array's device address.
+// (Host code only sees a host-side stand-in under the array's name.)
+int noalloc_setup(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(SMX_BAD_ARGUMENT, "device index out of range");
+    if (!g_noalloc_ptr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(SMX_CUDA_ERROR, std::string("cudaGetSymbolAddress(no-allocation scratch): ") +
+                                            cudaGetErrorString(e));
+        g_noalloc_ptr[device] = ptr;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+    return SMX_OK;
+}
+}  // namespace
+
+int device_enumerate_noalloc(smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order,
+                             const smx_enum_opts& o, uint64_t limit, volatile uint32_t* stop, smx_stats* st) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    SMX_CUDA_TRY(cudaSetDevice(g->device));
+    unsigned char* base = nullptr;
+    int rc = noalloc_setup(g->device, &base);
+    if (rc != SMX_OK) return rc;
+    cudaStream_t s = g->stream;
+    HostPlanBuild hb;
+    rc = build_host_plan(g, q, c, order, o.explore, o.lane_depth, o.bitmap_min >= 0, hb);
+    if (rc != SMX_OK) return rc;
+    const uint64_t scratch_elems = std::max<uint64_t>(8, hb.scratch_elems);
+    const uint64_t bm_words = hb.bm_words;
+    const uint32_t max_ops = std::max<uint32_t>(1, hb.plan.nops);
+    // layout of the array: control block | plan | bn / op / part pool | per-warp scratch | bitmaps
+    const size_t o_next = 0, o_status = 8, o_stats = 16, o_qcount = 64, o_qlimit = 72, o_prefix = 80, o_qstop = 96;
+    const size_t o_plan = 256;
+    const size_t o_pool = (o_plan + sizeof(QPlan) + 255) & ~(size_t)255;
+    size_t at = o_pool;
+    auto place = [&](size_t bytes) {
+        at = (at + 15) & ~(size_t)15;
+        const size_t off = at;
+        at += bytes;
+        return off;
+    };
+    const size_t o_bn = place(hb.bn.size() * sizeof(BnRef));
+    const size_t o_op = place(hb.op.size() * sizeof(OpInfo));
+    const size_t o_part = place(hb.part.size() * sizeof(PartRef));
+    const size_t o_scr = (at + 255) & ~(size_t)255;
+    // launch shape as smx_enumerate, with no more warps than the array holds
+    const uint32_t wpb = o.warps_per_block > 0 ? std::min<uint32_t>((uint32_t)o.warps_per_block, 8u) : 8u;
+    const uint32_t chunk = o.stage_chunk > 0 ? ((uint32_t)o.stage_chunk + 3) & ~3u : 1024u;
+    const size_t stage_bytes = ((size_t)(chunk + 8) * 4 + 15) & ~(size_t)15;
+    const size_t smem = stage_bytes * wpb + 16 * wpb + (size_t)max_ops * sizeof(OpState) * wpb;
+    if (smem > 227 * 1024)
+        return fail(SMX_TOO_LARGE, "shared memory per block above 227 KB: lower stage_chunk or warps_per_block");
+    auto kern = o.blocks_per_sm >= 3 ? enum_kernel<3> : enum_kernel<2>;
+    SMX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int bps = 0;
+    SMX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, (int)(wpb * 32), smem));
+    if (o.blocks_per_sm > 0) bps = std::min(bps, o.blocks_per_sm);
+    if (bps < 1) return fail(SMX_TOO_LARGE, "enumeration kernel does not fit on an SM with this shared-memory size");
+    const size_t per_warp = ((size_t)(scratch_elems + bm_words)) * 4;
+    const size_t per_block = per_warp * wpb;
+    const size_t cap = (size_t)SMX_NOALLOC_SCRATCH_BYTES;
+    if (o_scr + per_block + 512 > cap)
+        return fail(SMX_TOO_LARGE, "the query needs " + std::to_string(o_scr + per_block + 512) +
+                                       " bytes of working memory for one block of " + std::to_string(wpb) +
+                                       " warps; smx_enumerate_noalloc has " + std::to_string(cap) +
+                                       " (SMX_NOALLOC_SCRATCH_BYTES): use smx_enumerate or fewer warps_per_block");
+    const uint32_t blocks =
+        (uint32_t)std::min<size_t>((size_t)g->num_sms * bps, (cap - o_scr - 512) / per_block);
+    const uint64_t nwarps = (uint64_t)blocks * wpb;
+    const size_t o_bm = (o_scr + nwarps * scratch_elems * 4 + 255) & ~(size_t)255;
+    // control block (zeroed), limit, task prefix, plan and pool in one host image
+    std::vector<unsigned char> img(o_scr, 0);
+    std::memcpy(img.data() + o_qlimit, &limit, 8);
+    const uint64_t prefix[2] = {0, hb.plan.ntasks};
+    std::memcpy(img.data() + o_prefix, prefix, sizeof(prefix));
+    QPlan plan = hb.plan;
+    plan.bn = reinterpret_cast<const BnRef*>(base + o_bn);
+    plan.op = reinterpret_cast<const OpInfo*>(base + o_op);
+    plan.part = reinterpret_cast<const PartRef*>(base + o_part);
+    std::memcpy(img.data() + o_plan, &plan, sizeof(QPlan));
+    if (!hb.bn.empty()) std::memcpy(img.data() + o_bn, hb.bn.data(), hb.bn.size() * sizeof(BnRef));
+    if (!hb.op.empty()) std::memcpy(img.data() + o_op, hb.op.data(), hb.op.size() * sizeof(OpInfo));
+    if (!hb.part.empty()) std::memcpy(img.data() + o_part, hb.part.data(), hb.part.size() * sizeof(PartRef));
+    SMX_CUDA_TRY(cudaMemcpyAsync(base, img.data(), img.size(), cudaMemcpyHostToDevice, s));
+    const volatile uint32_t* d_host_stop = nullptr;
+    if (stop) {
+        void* dp = nullptr;
+        if (cudaHostGetDevicePointer(&dp, (void*)stop, 0) == cudaSuccess) d_host_stop = static_cast<const volatile uint32_t*>(dp);
+        else cudaGetLastError();
+    }
+    EnumArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.plans = reinterpret_cast<const QPlan*>(base + o_plan);
+    A.task_prefix = reinterpret_cast<const uint64_t*>(base + o_prefix);
+    A.next_task = reinterpret_cast<unsigned long long*>(base + o_next);
+    A.qcount = reinterpret_cast<unsigned long long*>(base + o_qcount);
+    A.qstop = reinterpret_cast<uint32_t*>(base + o_qstop);
+    A.qlimit = reinterpret_cast<const uint64_t*>(base + o_qlimit);
+    A.scratch = reinterpret_cast<uint32_t*>(base + o_scr);
+    A.stats = reinterpret_cast<unsigned long long*>(base + o_stats);
+    A.status = reinterpret_cast<int*>(base + o_status);
+    A.host_stop = d_host_stop;
+    A.scratch_stride = scratch_elems;
+    A.bitmap = bm_words ? reinterpret_cast<uint32_t*>(base + o_bm) : nullptr;
+    A.bm_stride = bm_words;
+    A.bitmap_min = o.bitmap_min > 0 ? (uint32_t)o.bitmap_min : 32u;
+    A.budget_ns = o.time_budget_ms > 0 ? (uint64_t)(o.time_budget_ms * 1e6) : 0;
+    A.nq = 1;
+    A.max_ops = max_ops;
+    A.grab = o.task_grab > 0 ? (uint32_t)o.task_grab : 4u;
+    A.chunk = chunk;
+    A.gallop_ratio = o.gallop_ratio > 0 ? (uint32_t)o.gallop_ratio : 16u;
+    A.use_tma = o.use_tma ? 1u : 0u;
+    A.failing_sets = o.failing_sets ? 1u : 0u;
+    const auto t0 = std::chrono::steady_clock::now();
+    SMX_LAUNCH(kern, blocks, wpb * 32, smem, s, A);
+    SMX_CUDA_TRY(cudaGetLastError());
+    unsigned char back[128];
+    SMX_CUDA_TRY(cudaMemcpyAsync(back, base, sizeof(back), cudaMemcpyDeviceToHost, s));
+    SMX_CUDA_TRY(cudaStreamSynchronize(s));
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    unsigned long long qc = 0, stats[5];
+    int status = 0;
+    std::memcpy(&qc, back + o_qcount, 8);
+    std::memcpy(stats, back + o_stats, sizeof(stats));
+    std::memcpy(&status, back + o_status, sizeof(int));
+    const bool reached = limit && qc >= limit;
+    if (st) {
+        st->count = reached ? limit : qc;
+        st->raw_count = qc;
+        st->intersections = stats[0];
+        st->nodes = stats[1];
+        st->bytes = stats[2];
+        st->tasks = stats[3];
+        st->pruned = stats[4];
+        st->kernel_ms = ms;
+        st->limit_reached = reached ? 1 : 0;
+        st->status = status;
+    }
+    if (status == SMX_CUDA_ERROR) return fail(SMX_CUDA_ERROR, "bulk copy wait did not complete; enumeration aborted");
+    if (status == SMX_TIMEOUT) set_error("time budget exhausted; the count is partial");
+    if (status == SMX_STOPPED) set_error("stopped by the caller; the count is partial");
+    return status;
 }
 
 }  // namespace smx

@@ -143,4 +143,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
                      const std::vector<uint64_t>& limits, volatile uint32_t* stop, uint64_t* counts,
                      smx_stats* st, bool use_graph);
 int ensure_scratch(smx_graph* g, size_t bytes);
+// smx_enumerate_noalloc: one query, all working memory in a file-scope device array
+int device_enumerate_noalloc(smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order,
+                             const smx_enum_opts& o, uint64_t limit, volatile uint32_t* stop, smx_stats* st);
 }  // namespace smx

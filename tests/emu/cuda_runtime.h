@@ -40,7 +40,7 @@
 #define __forceinline__ inline
 #define __launch_bounds__(...)
 #define __restrict__ __restrict
-#define __align__(n) alignas(n)
+#define __align__(n) __attribute__((aligned(n)))
 
 struct dim3 {
     unsigned x, y, z;
@@ -365,6 +365,11 @@ cudaError_t cudaFuncSetAttribute(F, cudaFuncAttribute, int) {
 template <class F>
 cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessor(int* n, F, int, size_t) {
     *n = 1;
+    return cudaSuccess;
+}
+template <class T>
+cudaError_t cudaGetSymbolAddress(void** p, const T& symbol) {
+    *p = (void*)&symbol;  // "device" variables are host variables here
     return cudaSuccess;
 }
 // typed overloads, as the CUDA runtime header provides for C++
