@@ -1761,11 +1761,18 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
 
 int ensure_scratch(smx_graph* g, size_t bytes) {
     if (g->scratch_bytes >= bytes) return SMX_OK;
+    // grow by at least half again, so a run of slightly larger queries does
+    // not reallocate every time; fall back to the exact size if that fails
+    size_t want = std::max(bytes, g->scratch_bytes + g->scratch_bytes / 2);
     if (g->d_scratch) SMX_CUDA_TRY(cudaFree(g->d_scratch));
     g->d_scratch = nullptr;
     g->scratch_bytes = 0;
-    SMX_CUDA_TRY(cudaMalloc(&g->d_scratch, bytes));
-    g->scratch_bytes = bytes;
+    if (cudaMalloc(&g->d_scratch, want) != cudaSuccess) {
+        cudaGetLastError();
+        want = bytes;
+        SMX_CUDA_TRY(cudaMalloc(&g->d_scratch, want));
+    }
+    g->scratch_bytes = want;
     return SMX_OK;
 }
 

@@ -593,6 +593,16 @@ int upload_graph(smx_graph* g) {
     SMX_CUDA_TRY(cudaSetDevice(g->device));
     SMX_CUDA_TRY(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
     SMX_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    {
+        // candidate sets and plans come from the device's default pool
+        // (cudaMallocAsync); keep freed blocks in the pool instead of returning
+        // them to the driver at every synchronisation, which costs up to a
+        // second per filter / destroy on large graphs
+        cudaMemPool_t pool;
+        SMX_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, g->device));
+        uint64_t keep = UINT64_MAX;
+        SMX_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     const HostGraph& h = g->h;
     cudaStream_t st = g->stream;
     SMX_CUDA_TRY(cudaMalloc(&g->d_off, (h.n + 1) * sizeof(uint64_t)));

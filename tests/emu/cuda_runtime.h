@@ -334,6 +334,13 @@ cudaError_t cudaMalloc(void** p, size_t n);
 cudaError_t cudaMallocAsync(void** p, size_t n, cudaStream_t s);
 cudaError_t cudaFree(void* p);
 cudaError_t cudaMemGetInfo(size_t* free_bytes, size_t* total_bytes);
+typedef struct EmuPool* cudaMemPool_t;
+enum cudaMemPoolAttr { cudaMemPoolAttrReleaseThreshold = 4 };
+inline cudaError_t cudaDeviceGetDefaultMemPool(cudaMemPool_t* p, int) {
+    *p = nullptr;
+    return 0;
+}
+inline cudaError_t cudaMemPoolSetAttribute(cudaMemPool_t, cudaMemPoolAttr, void*) { return 0; }
 cudaError_t cudaFreeAsync(void* p, cudaStream_t s);
 cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind k);
 cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind k, cudaStream_t st);
