@@ -125,12 +125,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM traffic of the enumeration kernel from the committed ncu summary, if any."""
+def ncu_traffic(launch_ms: float):
+    """DRAM bytes (read + write) of one enumeration launch of launch_ms: the
+    rate of the launch captured by ncu (profiles/enum_kernel_cfg2.json, a
+    smaller cap of the same workload, cold caches) scaled by device time."""
     path = os.path.join(ROOT, "profiles", "enum_kernel_cfg2.json")
-    if os.path.exists(path):
+    if os.path.exists(path) and launch_ms > 0:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            rate = json.load(f).get("dram_bytes_per_ms")
+        return rate * launch_ms if rate else None
     return None
 
 
@@ -268,6 +271,8 @@ def run_smx(args, world, rank, local, pg):
     build_tables = args.explore == 0
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
 
+    n_enum = [0]
+
     def step(graph, batch):
         embeddings = 0
         kernel_ms = 0.0
@@ -279,6 +284,7 @@ def run_smx(args, world, rank, local, pg):
                 embeddings += st.count
                 kernel_ms += st.kernel_ms
                 kbytes += st.bytes
+                n_enum[0] += 1
         return embeddings, kernel_ms, kbytes
 
     for i in range(args.warmup):
@@ -287,6 +293,7 @@ def run_smx(args, world, rank, local, pg):
     # ---- timed: device-resident inputs
     times, emb, kms, kby = [], 0, 0.0, 0
     launches0 = _lib.lib.smx_launch_count()
+    n_enum[0] = 0
     clocks = Clocks(dev)
     clocks.start()
     nq_timed = 0
@@ -308,6 +315,7 @@ def run_smx(args, world, rank, local, pg):
         kby += kb
     clock_info = clocks.stop()
     launches = _lib.lib.smx_launch_count() - launches0
+    enum_launches = n_enum[0]
     step_ms = max_over_ranks(pg, sum(times) / len(times))
     # ---- e2e: pinned host CSR -> device graph, queries, counts back, per step
     p_off = torch.from_numpy(off.view(np.int64)).pin_memory()
@@ -342,6 +350,7 @@ def run_smx(args, world, rank, local, pg):
     value = q_per_step / (step_ms / 1000.0)
     hbm, peak_kind = peaks()
     achieved = (kby / 1e9) / (kms / 1000.0) if kms > 0 else 0.0
+    launch_ms = kms / enum_launches if enum_launches else 0.0
     line = {
         "metric": METRIC,
         "value": value,
@@ -363,10 +372,12 @@ def run_smx(args, world, rank, local, pg):
         "e2e": {"value": q_per_step / (e2e_ms / 1000.0), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm if hbm else None, "traffic": ncu_traffic(),
+                     "frac": achieved / hbm if hbm else None, "traffic": ncu_traffic(launch_ms),
                      "kernel": "enum_kernel", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": kby / enum_launches if enum_launches else None,
                      "note": "achieved = algorithmic bytes (list elements touched x 4 + row/candidate reads) / "
-                             "event-timed kernel time, summed over the timed launches"},
+                             "event-timed kernel time, summed over the timed launches; traffic = DRAM bytes of "
+                             "an average timed launch, from the ncu capture's bytes per ms (cold caches)"},
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
