@@ -189,6 +189,40 @@ int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand
                         const uint32_t* const* orders, uint32_t nq, const smx_enum_opts* opts,
                         uint64_t limit, uint64_t* counts, smx_stats* out);
 
+/* ------------------------------------------------------------ learned matching order */
+/* No counterpart in the reference (its orders are rule-based, order.h:1138-1281,
+ * or analytic cost models, order.h:1391-1645).  A 64-256-256-1 MLP (ReLU, BF16
+ * weights and activations, FP32 accumulation; Adam on FP32 master weights)
+ * predicts the enumeration work of a (query, order) pair from
+ * smx_order_features; smx_order_learned picks the order of a beam with the
+ * smallest prediction.  An order never changes a count, only the work. */
+#define SMX_MLP_INPUTS 64
+#define SMX_MLP_HIDDEN 256
+/* parameters, fp32: W1[256][64] b1[256] W2[256][256] b2[256] W3[256] b3[1] */
+#define SMX_MLP_PARAMS 82689
+typedef struct smx_mlp smx_mlp;
+size_t smx_mlp_param_count(void);
+/* He-normal weights from `seed`; batches of 1..max_batch rows. */
+int smx_mlp_create(int device, uint32_t max_batch, uint64_t seed, smx_mlp** out);
+int smx_mlp_set_params(smx_mlp* m, const float* params, size_t n); /* also resets the Adam state */
+int smx_mlp_get_params(const smx_mlp* m, float* params, size_t n);
+/* y[i] = model(x[i]) for n rows of SMX_MLP_INPUTS floats (host buffers). */
+int smx_mlp_forward(smx_mlp* m, const float* x, uint32_t n, float* y);
+/* Gradients of sum_i (y_i - t_i)^2 / (2n) in the parameter layout, and that loss; no update. */
+int smx_mlp_gradients(smx_mlp* m, const float* x, const float* t, uint32_t n, float* grads, float* loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on that loss; *loss = loss before the step. */
+int smx_mlp_train_step(smx_mlp* m, const float* x, const float* t, uint32_t n, float lr, float* loss);
+void smx_mlp_destroy(smx_mlp* m);
+/* The model's 64 inputs for `order` (valid order of q; candidate counts from c). */
+int smx_order_features(const smx_query* q, const smx_cand* c, const uint32_t* order, float* out);
+/* Up to `beam` distinct valid orders into orders[beam][n]: RI, GQL, then seeded
+ * randomized greedy orders; *produced = how many. */
+int smx_order_beam(const smx_query* q, const smx_cand* c, uint32_t beam, uint64_t seed, uint32_t* orders,
+                   uint32_t* produced);
+/* The beam order with the smallest predicted work (beam <= the model's max_batch). */
+int smx_order_learned(smx_mlp* m, const smx_query* q, const smx_cand* c, uint32_t beam, uint64_t seed,
+                      uint32_t* order, float* predicted);
+
 /* ------------------------------------------------------------ enumeration without allocation */
 /* No counterpart in the reference.  smx_enumerate allocates device memory on
  * every call (its plans, and scratch that grows with the query); some callers

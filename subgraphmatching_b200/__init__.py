@@ -475,3 +475,96 @@ def explore_batch(data: Graph, queries, cans, orders=None, opts: EnumOptions | N
     out = Stats.from_c(st)
     out.status = rc
     return [int(x) for x in counts[:nq]], out
+
+
+# ---------------------------------------------------------------------- learned order
+MLP_INPUTS = 64
+MLP_PARAMS = 82689
+
+
+def _pf(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class MLP:
+    """The learned-order cost model on a device (smx_mlp_*): 64-256-256-1,
+    ReLU, BF16 weights / activations, FP32 accumulation, Adam on FP32 masters.
+    No counterpart in the reference."""
+
+    def __init__(self, device: int = 0, max_batch: int = 4096, seed: int = 0):
+        h = ctypes.c_void_p()
+        check(lib.smx_mlp_create(device, max_batch, seed, ctypes.byref(h)))
+        self._h = h
+        self.max_batch = max_batch
+
+    def __del__(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.smx_mlp_destroy(self._h)
+            self._h = None
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_PARAMS, dtype=np.float32)
+        check(lib.smx_mlp_get_params(self._h, _pf(p), MLP_PARAMS))
+        return p
+
+    @params.setter
+    def params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib.smx_mlp_set_params(self._h, _pf(p), len(p)))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_INPUTS)
+        y = np.zeros(len(x), dtype=np.float32)
+        for i in range(0, len(x), self.max_batch):
+            xs = np.ascontiguousarray(x[i:i + self.max_batch])
+            ys = np.zeros(len(xs), dtype=np.float32)
+            check(lib.smx_mlp_forward(self._h, _pf(xs), len(xs), _pf(ys)))
+            y[i:i + len(xs)] = ys
+        return y
+
+    def gradients(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_INPUTS)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(MLP_PARAMS, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        check(lib.smx_mlp_gradients(self._h, _pf(x), _pf(t), len(x), _pf(g), _pf(loss)))
+        return g, float(loss[0])
+
+    def train_step(self, x, t, lr: float = 1e-3) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_INPUTS)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        check(lib.smx_mlp_train_step(self._h, _pf(x), _pf(t), len(x), float(lr), _pf(loss)))
+        return float(loss[0])
+
+    def save(self, path: str) -> None:
+        np.save(path, self.params)
+
+    def load(self, path: str) -> None:
+        self.params = np.load(path)
+
+
+def order_features(query: Query, can: CandidateParam, order) -> np.ndarray:
+    o = np.ascontiguousarray(order, dtype=np.uint32)
+    f = np.zeros(MLP_INPUTS, dtype=np.float32)
+    check(lib.smx_order_features(query._h, can._h, _p32(o), _pf(f)))
+    return f
+
+
+def order_beam(query: Query, can: CandidateParam, beam: int = 32, seed: int = 0) -> list[list[int]]:
+    """RI, GQL and seeded randomized greedy orders (distinct, valid)."""
+    n = query.getVertexCnt()
+    out = np.zeros(beam * n, dtype=np.uint32)
+    k = ctypes.c_uint32()
+    check(lib.smx_order_beam(query._h, can._h, beam, seed, _p32(out), ctypes.byref(k)))
+    return [[int(v) for v in out[i * n:(i + 1) * n]] for i in range(k.value)]
+
+
+def Order_Learned(model: MLP, query: Query, can: CandidateParam, beam: int = 32, seed: int = 0) -> list[int]:
+    """The beam order with the smallest predicted enumeration work."""
+    n = query.getVertexCnt()
+    out = np.zeros(n, dtype=np.uint32)
+    pred = ctypes.c_float()
+    check(lib.smx_order_learned(model._h, query._h, can._h, beam, seed, _p32(out), ctypes.byref(pred)))
+    return [int(v) for v in out]

@@ -71,6 +71,7 @@ _dbl = ctypes.c_double
 _pu32 = ctypes.POINTER(ctypes.c_uint32)
 _pu64 = ctypes.POINTER(ctypes.c_uint64)
 _str = ctypes.c_char_p
+_pf = ctypes.POINTER(ctypes.c_float)
 
 # (name, restype, argtypes) for every entry point of include/smx.h
 SIGNATURES = [
@@ -109,6 +110,17 @@ SIGNATURES = [
     ("smx_enumerate", _i32, [_vp, _vp, _vp, _pu32, ctypes.POINTER(EnumOpts), _u64, _pu32, ctypes.POINTER(StatsC)]),
     ("smx_enumerate_noalloc", _i32, [_vp, _vp, _vp, _pu32, ctypes.POINTER(EnumOpts), _u64, _pu32,
                                      ctypes.POINTER(StatsC)]),
+    ("smx_mlp_param_count", ctypes.c_size_t, []),
+    ("smx_mlp_create", _i32, [_i32, _u32, _u64, _pvp]),
+    ("smx_mlp_set_params", _i32, [_vp, _pf, ctypes.c_size_t]),
+    ("smx_mlp_get_params", _i32, [_vp, _pf, ctypes.c_size_t]),
+    ("smx_mlp_forward", _i32, [_vp, _pf, _u32, _pf]),
+    ("smx_mlp_gradients", _i32, [_vp, _pf, _pf, _u32, _pf, _pf]),
+    ("smx_mlp_train_step", _i32, [_vp, _pf, _pf, _u32, ctypes.c_float, _pf]),
+    ("smx_mlp_destroy", None, [_vp]),
+    ("smx_order_features", _i32, [_vp, _vp, _pu32, _pf]),
+    ("smx_order_beam", _i32, [_vp, _vp, _u32, _u64, _pu32, _pu32]),
+    ("smx_order_learned", _i32, [_vp, _vp, _vp, _u32, _u64, _pu32, _pf]),
     ("smx_stop_flag_create", _i32, [_i32, ctypes.POINTER(_pu32)]),
     ("smx_stop_flag_destroy", None, [_pu32]),
     ("smx_enumerate_batch", _i32, [_vp, _pvp, _pvp, ctypes.POINTER(_pu32), _u32, ctypes.POINTER(EnumOpts), _u64,

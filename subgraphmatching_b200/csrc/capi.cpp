@@ -332,6 +332,47 @@ int smx_order_gql(const smx_query* q, const smx_cand* c, uint32_t* order) {
     return SMX_OK;
 }
 
+int smx_order_features(const smx_query* q, const smx_cand* c, const uint32_t* order, float* out) {
+    if (!q || !c || !order || !out) return fail(SMX_BAD_ARGUMENT, "null argument");
+    if (c->qn != q->h.n) return fail(SMX_BAD_ARGUMENT, "candidates belong to another query");
+    if (!order_valid(q->h, order)) return fail(SMX_INVALID_ORDER, "order is not a connected permutation of the query vertices");
+    order_features(q->h, c->cnt.data(), order, out);
+    return SMX_OK;
+}
+
+int smx_order_beam(const smx_query* q, const smx_cand* c, uint32_t beam, uint64_t seed, uint32_t* orders,
+                   uint32_t* produced) {
+    if (!q || !c || !orders || !produced) return fail(SMX_BAD_ARGUMENT, "null argument");
+    if (c->qn != q->h.n) return fail(SMX_BAD_ARGUMENT, "candidates belong to another query");
+    if (!c->g) return fail(SMX_BAD_ARGUMENT, "the candidate set's data graph was destroyed");
+    std::vector<std::vector<uint32_t>> out;
+    order_beam(q->h, c->cnt.data(), c->g->h.n, beam, seed, out);
+    for (size_t i = 0; i < out.size(); ++i) std::copy(out[i].begin(), out[i].end(), orders + i * q->h.n);
+    *produced = (uint32_t)out.size();
+    return SMX_OK;
+}
+
+int smx_order_learned(smx_mlp* m, const smx_query* q, const smx_cand* c, uint32_t beam, uint64_t seed,
+                      uint32_t* order, float* predicted) {
+    if (!m || !q || !c || !order) return fail(SMX_BAD_ARGUMENT, "null argument");
+    if (beam == 0) return fail(SMX_BAD_ARGUMENT, "beam must be at least 1");
+    const uint32_t n = q->h.n;
+    std::vector<uint32_t> orders((size_t)beam * n);
+    uint32_t k = 0;
+    int rc = smx_order_beam(q, c, beam, seed, orders.data(), &k);
+    if (rc != SMX_OK) return rc;
+    std::vector<float> x((size_t)k * SMX_MLP_INPUTS), y(k);
+    for (uint32_t i = 0; i < k; ++i) order_features(q->h, c->cnt.data(), orders.data() + (size_t)i * n, x.data() + (size_t)i * SMX_MLP_INPUTS);
+    rc = smx_mlp_forward(m, x.data(), k, y.data());
+    if (rc != SMX_OK) return rc;
+    uint32_t best = 0;
+    for (uint32_t i = 1; i < k; ++i)
+        if (y[i] < y[best]) best = i;
+    std::copy(orders.begin() + (size_t)best * n, orders.begin() + (size_t)(best + 1) * n, order);
+    if (predicted) *predicted = y[best];
+    return SMX_OK;
+}
+
 int smx_order_valid(const smx_query* q, const uint32_t* order) {
     if (!q || !order) return 0;
     return order_valid(q->h, order) ? 1 : 0;

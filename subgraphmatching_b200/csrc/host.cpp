@@ -581,6 +581,115 @@ void order_gql(const HostQuery& q, const uint32_t* cnt, uint32_t data_n, uint32_
     }
 }
 
+// ------------------------------------------------------------------ learned order: features and beam
+// Features of a (query, order) pair for the cost model (64 floats, all
+// roughly in [0, 2]): query size and degree / core statistics, per position
+// (first 24) the log candidate count and the number of backward neighbours,
+// and the cumulative estimated log tree size at positions 1, 2, 3, 4, 6, 8,
+// 12, 16 (log candidate count minus 4 bits per extra backward neighbour).
+void order_features(const HostQuery& q, const uint32_t* cnt, const uint32_t* order, float* f) {
+    const uint32_t n = q.n;
+    for (int i = 0; i < SMX_MLP_INPUTS; ++i) f[i] = 0.f;
+    std::vector<uint32_t> core;
+    kcore(q, core);
+    uint32_t maxc = 0, maxd = 0;
+    double sumc = 0, suml = 0, minl = 1e30;
+    for (uint32_t u = 0; u < n; ++u) {
+        maxc = std::max(maxc, core[u]);
+        sumc += core[u];
+        maxd = std::max(maxd, q.deg(u));
+        const double l = std::log2(1.0 + cnt[u]);
+        suml += l;
+        minl = std::min(minl, l);
+    }
+    f[0] = n / 32.f;
+    f[1] = q.m / 64.f;
+    f[2] = n ? (2.f * q.m / n) / 8.f : 0.f;
+    f[3] = maxd / 16.f;
+    f[4] = maxc / 8.f;
+    f[5] = n ? (float)(sumc / n) / 8.f : 0.f;
+    f[6] = n ? (float)(suml / n) / 20.f : 0.f;
+    f[7] = n ? (float)minl / 20.f : 0.f;
+    uint64_t seen = 0;
+    std::vector<double> est(n, 0.0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t u = order[i];
+        const uint32_t nbn = (uint32_t)__builtin_popcountll(q.nbr_mask[u] & seen);
+        const double l = std::log2(1.0 + cnt[u]);
+        if (i < 24) {
+            f[8 + i] = (float)l / 20.f;
+            f[32 + i] = nbn / 8.f;
+        }
+        est[i] = std::max(0.0, l - 4.0 * (nbn > 0 ? nbn - 1 : 0));
+        seen |= 1ull << u;
+    }
+    const uint32_t at[8] = {1, 2, 3, 4, 6, 8, 12, 16};
+    for (int k = 0; k < 8; ++k) {
+        double c = 0;
+        for (uint32_t i = 0; i < std::min(at[k], n); ++i) c += est[i];
+        f[56 + k] = (float)c / 64.f;
+    }
+}
+
+// Candidate orders: RI, GQL, then randomized greedy orders (start drawn with
+// weight 1 / (1 + |C(u)|), each next vertex the frontier vertex with the best
+// score "2 x backward neighbours - log2 |C| / 4 + noise"), without repeats.
+void order_beam(const HostQuery& q, const uint32_t* cnt, uint32_t data_n, uint32_t beam, uint64_t seed,
+                std::vector<std::vector<uint32_t>>& out) {
+    const uint32_t n = q.n;
+    out.clear();
+    auto add = [&](const std::vector<uint32_t>& o) {
+        for (const auto& x : out)
+            if (x == o) return;
+        out.push_back(o);
+    };
+    std::vector<uint32_t> o(n);
+    order_ri(q, o.data());
+    if (beam > out.size()) add(o);
+    order_gql(q, cnt, data_n, o.data());
+    if (beam > out.size()) add(o);
+    uint64_t st = seed * 0x9e3779b97f4a7c15ULL + 0x1234567ULL;
+    auto rnd = [&]() {
+        st += 0x9e3779b97f4a7c15ULL;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+        return ((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (uint32_t attempt = 0; out.size() < beam && attempt < 8 * beam + 16; ++attempt) {
+        double tot = 0;
+        for (uint32_t u = 0; u < n; ++u) tot += 1.0 / (1.0 + cnt[u]);
+        double r = rnd() * tot;
+        uint32_t s = n - 1;
+        for (uint32_t u = 0; u < n; ++u) {
+            r -= 1.0 / (1.0 + cnt[u]);
+            if (r <= 0) {
+                s = u;
+                break;
+            }
+        }
+        const double noise = 0.5 + 2.0 * rnd();
+        uint64_t seen = 1ull << s;
+        o[0] = s;
+        for (uint32_t i = 1; i < n; ++i) {
+            double best = -1e300;
+            uint32_t pick = n;
+            for (uint32_t u = 0; u < n; ++u) {
+                if (((seen >> u) & 1) || !(q.nbr_mask[u] & seen)) continue;
+                const double sc = 2.0 * __builtin_popcountll(q.nbr_mask[u] & seen) -
+                                  std::log2(1.0 + cnt[u]) / 4.0 + noise * rnd();
+                if (sc > best) {
+                    best = sc;
+                    pick = u;
+                }
+            }
+            o[i] = pick;
+            seen |= 1ull << pick;
+        }
+        add(o);
+    }
+}
+
 // isValid (order.h:104-124) plus a permutation check.
 bool order_valid(const HostQuery& q, const uint32_t* order) {
     uint64_t seen = 0;

@@ -63,6 +63,9 @@ void kcore(const HostQuery& q, std::vector<uint32_t>& core);
 void order_ri(const HostQuery& q, uint32_t* order);
 void order_gql(const HostQuery& q, const uint32_t* cand_counts, uint32_t data_n, uint32_t* order);
 bool order_valid(const HostQuery& q, const uint32_t* order);
+void order_features(const HostQuery& q, const uint32_t* cnt, const uint32_t* order, float* out);
+void order_beam(const HostQuery& q, const uint32_t* cnt, uint32_t data_n, uint32_t beam, uint64_t seed,
+                std::vector<std::vector<uint32_t>>& out);
 
 // PlanIR (code_gen.h:682-847): deduplicated prefix-intersection ops.
 struct PlanOp {
