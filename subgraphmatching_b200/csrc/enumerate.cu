@@ -1353,7 +1353,13 @@ __global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
                 qlo = A.task_prefix[q];
                 qhi = A.task_prefix[q + 1];
             }
-            if (query_stopped(A, q)) continue;
+            if (query_stopped(A, q)) {
+                // the query reached its limit: move the queue past its tasks
+                // instead of draining them one grab at a time
+                if (lane == 0) atomicMax(A.next_task, (unsigned long long)qhi);
+                t = qhi - 1;
+                continue;
+            }
             const QPlan& P = A.plans[q];
             T.q = q;
             T.local = 0;
@@ -1680,6 +1686,9 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     A.nq = nq;
     A.max_ops = max_ops;
     A.grab = o.task_grab > 0 ? (uint32_t)o.task_grab : 4u;
+    // many light tasks: larger grabs, so the queue's one counter is not the
+    // bottleneck (each warp still takes >= 256 grabs on average)
+    A.grab = (uint32_t)std::max<uint64_t>(A.grab, std::min<uint64_t>(prefix[nq] / (nwarps * 256), 1024));
     A.chunk = chunk;
     A.gallop_ratio = o.gallop_ratio > 0 ? (uint32_t)o.gallop_ratio : 16u;
     A.use_tma = o.use_tma ? 1u : 0u;

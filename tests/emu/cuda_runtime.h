@@ -296,6 +296,12 @@ inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }
 inline unsigned long long atomicAnd(unsigned long long* p, unsigned long long v) {
     return __atomic_fetch_and(p, v, __ATOMIC_SEQ_CST);
 }
+inline unsigned long long atomicMax(unsigned long long* p, unsigned long long v) {
+    unsigned long long cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+    while (cur < v && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
+    }
+    return cur;
+}
 inline unsigned atomicMax(unsigned* p, unsigned v) {
     unsigned cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
     while (cur < v && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
