@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--cap", type=int, default=CAP)
     ap.add_argument("--explore", type=int, default=0, help="0 candidate tables, 1 cache + failing sets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", type=int, default=2, choices=[2, 4],
+                    help="2: the headline workload; 4: learned order + batched launch vs RI order one query at a time")
+    ap.add_argument("--chunk", type=int, default=50, help="--config 4: queries per batched launch")
+    ap.add_argument("--train-queries", type=int, default=120, help="--config 4: queries that train the order model")
     return ap.parse_args()
 
 
@@ -391,12 +395,109 @@ def run_smx(args, world, rank, local, pg):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------- config 4
+C4_VERT, C4_EDGE, C4_SEED = 4_000_000, 40_000_000, 4
+C4_CAP, C4_BUDGET_MS = 100_000_000, 2000.0
+
+
+def c4_specs(n: int, base: int):
+    """(k, dense, seed): sizes uniform in 4..32 (seeded), dense and sparse alternating."""
+    import numpy as np
+
+    rng = np.random.default_rng(base)
+    return [(int(rng.integers(4, 33)), i % 2 == 0, base + i) for i in range(n)]
+
+
+def run_cfg4(args, world, rank, local, pg):
+    """Learned order + one batched persistent launch per chunk (autotuned
+    settings) against RI order with one launch per query, on the same
+    filtered candidates; counts must agree wherever neither run hit the time
+    budget.  Filtering is timed separately (it is the same for both)."""
+    import numpy as np
+
+    import subgraphmatching_b200 as smx
+    from subgraphmatching_b200 import autotune as at
+    from subgraphmatching_b200 import learned_order as lo
+
+    dev = local
+    t0 = time.perf_counter()
+    hg = smx.Graph.generate(C4_VERT, C4_EDGE, GAMMA, 1, 1.0, C4_SEED, device=-1)
+    off, nb, lab = hg.csr()
+    dg = smx.Graph.from_csr(off, nb, lab, device=dev)
+    nq = args.queries
+    queries = [smx.Query.generate(hg, k, d, s) for k, d, s in c4_specs(nq, 1_000_000 + rank * 100_000)]
+    train_q = [smx.Query.generate(hg, k, d, s) for k, d, s in c4_specs(args.train_queries, 2_000_000)]
+    setup_s = time.perf_counter() - t0
+    # the order model, trained on queries of its own
+    t0 = time.perf_counter()
+    samples = lo.collect(dg, train_q, beam=8, cap=10_000_000, budget_ms=300.0)
+    model = smx.MLP(dev, 1024, seed=7)
+    lo.train(model, samples, epochs=60, batch=128, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    # autotuned launch settings on a sample chunk
+    sample = queries[: min(20, nq)]
+    cans = [smx.CandidateParam(dg, q) for q in sample]
+    oks = [smx.Filter_GQL(dg, q, c) for q, c in zip(sample, cans)]
+    best, report = at.autotune(dg, [q for q, ok in zip(sample, oks) if ok], [c for c, ok in zip(cans, oks) if ok],
+                               cap=C4_CAP, budget_ms=C4_BUDGET_MS, repeats=1)
+    best.time_budget_ms = C4_BUDGET_MS
+    del cans
+    ri_ms = bl_ms = filt_s = 0.0
+    ri_dev = bl_dev = 0.0
+    mismatches = compared = timeouts = 0
+    for c0 in range(0, nq, args.chunk):
+        chunk = queries[c0:c0 + args.chunk]
+        t = time.perf_counter()
+        cans = [smx.CandidateParam(dg, q) for q in chunk]
+        oks = [smx.Filter_GQL(dg, q, c) for q, c in zip(chunk, cans)]
+        filt_s += time.perf_counter() - t
+        qs = [q for q, ok in zip(chunk, oks) if ok]
+        cs = [c for c, ok in zip(cans, oks) if ok]
+        # RI order, one launch per query
+        t = time.perf_counter()
+        ri = [smx.explore(dg, q, c, None, smx.EnumOptions(time_budget_ms=C4_BUDGET_MS), C4_CAP) for q, c in zip(qs, cs)]
+        ri_ms += (time.perf_counter() - t) * 1000.0
+        ri_dev += sum(r.kernel_ms for r in ri)
+        # learned order (inference included) + one batched launch
+        t = time.perf_counter()
+        orders = [smx.Order_Learned(model, q, c, 32, 7) for q, c in zip(qs, cs)]
+        counts, st = smx.explore_batch(dg, qs, cs, orders, best, C4_CAP)
+        bl_ms += (time.perf_counter() - t) * 1000.0
+        bl_dev += st.kernel_ms
+        if st.status == 0:
+            for r, c in zip(ri, counts):
+                if r.status == 0:
+                    compared += 1
+                    mismatches += r.count != c
+        timeouts += sum(r.status != 0 for r in ri) + (st.status != 0)
+        del cans, cs
+    if rank != 0:
+        return
+    line = {
+        "metric": "queries/s: learned order + batched persistent launch vs RI order, one launch per query",
+        "value": nq / (bl_ms / 1000.0), "unit": "queries/s", "n_gpus": world, "higher_is_better": True,
+        "ri_single_value": nq / (ri_ms / 1000.0),
+        "speedup_vs_ri_single": ri_ms / bl_ms if bl_ms else None,
+        "device_ms": {"ri_single": ri_dev, "learned_batched": bl_dev},
+        "counts": {"compared": compared, "mismatches": mismatches, "runs_at_time_budget": timeouts},
+        "dtype": "u32", "data": "synthetic (seeded Chung-Lu graph and queries)",
+        "config": {"workload": f"cfg4: Chung-Lu {C4_VERT:,} V / {C4_EDGE:,} E (gamma {GAMMA}), {nq} queries of "
+                               f"4-32 vertices (half dense), GQL, cap {C4_CAP:.0e}, budget {C4_BUDGET_MS:.0f} ms",
+                   "chunk": args.chunk, "train_queries": args.train_queries, "train_samples": int(len(samples.t)),
+                   "autotuned": report["best"]},
+        "seconds": {"setup": setup_s, "train": train_s, "filter": filt_s},
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_init(args)
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, pg)
+        elif args.config == 4:
+            run_cfg4(args, world, rank, local, pg)
         else:
             run_smx(args, world, rank, local, pg)
     finally:
