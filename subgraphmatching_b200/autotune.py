@@ -32,6 +32,9 @@ GRID = [
     dict(blocks_per_sm=3),
 ]
 
+# the cache + failing-set explorer has no last-depth bitmap
+GRID_CACHE = [g for g in GRID if "bitmap_min" not in g]
+
 
 def autotune(graph, queries, cans, orders=None, cap: int = 0, budget_ms: float = 0.0, explore: int = 0,
              grid=None, repeats: int = 2, path: str | None = None) -> tuple[EnumOptions, dict]:

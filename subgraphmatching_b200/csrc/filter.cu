@@ -595,12 +595,14 @@ int upload_graph(smx_graph* g) {
     SMX_CUDA_TRY(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     {
         // candidate sets and plans come from the device's default pool
-        // (cudaMallocAsync); keep freed blocks in the pool instead of returning
-        // them to the driver at every synchronisation, which costs up to a
-        // second per filter / destroy on large graphs
+        // (cudaMallocAsync); keep up to 8 GB of freed blocks in the pool
+        // instead of returning them to the driver at every synchronisation,
+        // which costs up to a second per filter / destroy on large graphs
+        // (beyond 8 GB the pool gives memory back, so plain cudaMalloc of the
+        // enumeration scratch still finds it)
         cudaMemPool_t pool;
         SMX_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, g->device));
-        uint64_t keep = UINT64_MAX;
+        uint64_t keep = 8ull << 30;
         SMX_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     }
     const HostGraph& h = g->h;
