@@ -444,6 +444,7 @@ def run_cfg4(args, world, rank, local, pg):
     best, report = at.autotune(dg, [q for q, ok in zip(sample, oks) if ok], [c for c, ok in zip(cans, oks) if ok],
                                cap=C4_CAP, budget_ms=C4_BUDGET_MS, explore=1, repeats=1, grid=at.GRID_CACHE)
     best.time_budget_ms = C4_BUDGET_MS
+    best.budget_per_query = 1  # the same budget per query as the single launches
     del cans
     ri_ms = bl_ms = filt_s = 0.0
     ri_dev = bl_dev = 0.0
@@ -468,12 +469,11 @@ def run_cfg4(args, world, rank, local, pg):
         counts, st = smx.explore_batch(dg, qs, cs, orders, best, C4_CAP)
         bl_ms += (time.perf_counter() - t) * 1000.0
         bl_dev += st.kernel_ms
-        if st.status == 0:
-            for r, c in zip(ri, counts):
-                if r.status == 0:
-                    compared += 1
-                    mismatches += r.count != c
-        timeouts += sum(r.status != 0 for r in ri) + (st.status != 0)
+        for r, c, s_ in zip(ri, counts, st.query_status):
+            if r.status == 0 and s_ == 0:
+                compared += 1
+                mismatches += r.count != c
+        timeouts += sum(r.status != 0 for r in ri) + sum(s_ != 0 for s_ in st.query_status)
         del cans, cs
     if rank != 0:
         return
@@ -483,7 +483,7 @@ def run_cfg4(args, world, rank, local, pg):
         "ri_single_value": nq / (ri_ms / 1000.0),
         "speedup_vs_ri_single": ri_ms / bl_ms if bl_ms else None,
         "device_ms": {"ri_single": ri_dev, "learned_batched": bl_dev},
-        "counts": {"compared": compared, "mismatches": mismatches, "runs_at_time_budget": timeouts},
+        "counts": {"compared": compared, "mismatches": mismatches, "query_runs_at_time_budget": timeouts},
         "dtype": "u32", "data": "synthetic (seeded Chung-Lu graph and queries)",
         "config": {"workload": f"cfg4: Chung-Lu {C4_VERT:,} V / {C4_EDGE:,} E (gamma {GAMMA}), {nq} queries of "
                                f"4-32 vertices (half dense), GQL, cache + failing-set explorer, cap {C4_CAP:.0e}, budget {C4_BUDGET_MS:.0f} ms",

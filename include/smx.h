@@ -72,6 +72,9 @@ typedef struct {
     int32_t lane_depth;       /* candidate-table mode: depth (>= 2) from which each lane enumerates a
                                  subtree of its own; 0 = off (default), -1 = chosen from the query */
     double time_budget_ms;    /* 0 = unlimited; on expiry SMX_TIMEOUT with a partial count */
+    int32_t budget_per_query; /* smx_enumerate_batch: 1 = the budget applies to each query from its first
+                                 task (per-query status SMX_TIMEOUT), 0 = to the whole launch */
+    int32_t reserved0;
 } smx_enum_opts;
 
 /* Per-call statistics (the reference's Profiler counters, common_type.h:185-189,
@@ -184,10 +187,10 @@ void smx_stop_flag_destroy(volatile uint32_t* flag);
 /* Many queries against one data graph in one persistent work-stealing launch,
  * captured in a CUDA graph and replayed.  orders may be NULL (RI) or hold nq
  * pointers (NULL entries = RI).  counts[nq] out (min(count, limit) each); stats
- * aggregate. */
+ * aggregate; query_status[nq] (may be NULL) out: SMX_OK or SMX_TIMEOUT per query. */
 int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand* const* cs,
                         const uint32_t* const* orders, uint32_t nq, const smx_enum_opts* opts,
-                        uint64_t limit, uint64_t* counts, smx_stats* out);
+                        uint64_t limit, uint64_t* counts, smx_stats* out, int32_t* query_status);
 
 /* ------------------------------------------------------------ learned matching order */
 /* No counterpart in the reference (its orders are rule-based, order.h:1138-1281,

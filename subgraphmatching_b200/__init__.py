@@ -355,12 +355,13 @@ class EnumOptions:
     failing_sets: int = 1
     lane_depth: int = 0
     time_budget_ms: float = 0.0
+    budget_per_query: int = 0
 
     def to_c(self):
         o = _lib.EnumOpts()
         lib.smx_enum_opts_default(ctypes.byref(o))
         for k in ("explore", "warps_per_block", "blocks_per_sm", "task_grab", "stage_chunk", "gallop_ratio",
-                  "bitmap_min", "use_tma", "failing_sets", "lane_depth"):
+                  "bitmap_min", "use_tma", "failing_sets", "lane_depth", "budget_per_query"):
             setattr(o, k, int(getattr(self, k)))
         o.time_budget_ms = float(self.time_budget_ms)
         return o
@@ -378,6 +379,7 @@ class Stats:
     kernel_ms: float = 0.0
     limit_reached: bool = False
     status: int = 0
+    query_status: list | None = None  # explore_batch: SMX_OK / SMX_TIMEOUT per query
 
     @classmethod
     def from_c(cls, s) -> "Stats":
@@ -466,14 +468,16 @@ def explore_batch(data: Graph, queries, cans, orders=None, opts: EnumOptions | N
                 keep.append(a)
                 os_[i] = _p32(a)
     counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    qstat = np.zeros(max(nq, 1), dtype=np.int32)
     st = _lib.StatsC()
     o = opts.to_c()
     rc = lib.smx_enumerate_batch(data._h, qs, cs, os_, nq, ctypes.byref(o), output_limit, _p64(counts),
-                                 ctypes.byref(st))
+                                 ctypes.byref(st), qstat.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
     if rc not in (_lib.SMX_OK, _lib.SMX_TIMEOUT, _lib.SMX_STOPPED):
         check(rc)
     out = Stats.from_c(st)
     out.status = rc
+    out.query_status = [int(x) for x in qstat[:nq]]
     return [int(x) for x in counts[:nq]], out
 
 

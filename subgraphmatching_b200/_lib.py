@@ -44,6 +44,8 @@ class EnumOpts(ctypes.Structure):
         ("failing_sets", ctypes.c_int32),
         ("lane_depth", ctypes.c_int32),
         ("time_budget_ms", ctypes.c_double),
+        ("budget_per_query", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
     ]
 
 
@@ -124,7 +126,7 @@ SIGNATURES = [
     ("smx_stop_flag_create", _i32, [_i32, ctypes.POINTER(_pu32)]),
     ("smx_stop_flag_destroy", None, [_pu32]),
     ("smx_enumerate_batch", _i32, [_vp, _pvp, _pvp, ctypes.POINTER(_pu32), _u32, ctypes.POINTER(EnumOpts), _u64,
-                                   _pu64, ctypes.POINTER(StatsC)]),
+                                   _pu64, ctypes.POINTER(StatsC), ctypes.POINTER(ctypes.c_int32)]),
 ]
 
 

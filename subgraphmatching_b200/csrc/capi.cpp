@@ -554,9 +554,11 @@ void smx_stop_flag_destroy(volatile uint32_t* flag) {
 
 int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand* const* cs,
                         const uint32_t* const* orders, uint32_t nq, const smx_enum_opts* opts, uint64_t limit,
-                        uint64_t* counts, smx_stats* out) {
+                        uint64_t* counts, smx_stats* out, int32_t* query_status) {
     if (!g || (nq && (!qs || !cs))) return fail(SMX_BAD_ARGUMENT, "null argument");
     if (out) std::memset(out, 0, sizeof(*out));
+    if (query_status)
+        for (uint32_t i = 0; i < nq; ++i) query_status[i] = SMX_OK;
     smx_enum_opts o;
     if (opts) o = *opts; else smx_enum_opts_default(&o);
     std::vector<std::vector<uint32_t>> ords(nq);
@@ -588,9 +590,12 @@ int smx_enumerate_batch(smx_graph* g, const smx_query* const* qs, const smx_cand
     }
     if (hq.empty()) return SMX_OK;
     std::vector<uint64_t> cnt(hq.size(), 0);
-    int rc = device_enumerate(g, hq, hc, ho, o, lim, nullptr, cnt.data(), out, true);
-    if (counts)
-        for (size_t i = 0; i < slot.size(); ++i) counts[slot[i]] = cnt[i];
+    std::vector<int32_t> qst(hq.size(), SMX_OK);
+    int rc = device_enumerate(g, hq, hc, ho, o, lim, nullptr, cnt.data(), out, true, qst.data());
+    for (size_t i = 0; i < slot.size(); ++i) {
+        if (counts) counts[slot[i]] = cnt[i];
+        if (query_status) query_status[slot[i]] = qst[i];
+    }
     return rc;
 }
 

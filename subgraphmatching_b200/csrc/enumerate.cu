@@ -120,6 +120,7 @@ struct EnumArgs {
     uint32_t* scratch;              // per warp lists
     unsigned long long* stats;      // [0] intersections [1] nodes [2] bytes [3] tasks [4] pruned
     int* status;                    // 0 ok, SMX_TIMEOUT, SMX_STOPPED, SMX_CUDA_ERROR
+    unsigned long long* qstart;     // per query: %globaltimer when its first task began (per-query budgets)
     const volatile uint32_t* host_stop;
     uint64_t scratch_stride;        // elements per warp
     uint32_t* bitmap;               // per warp membership bitmap of the last depth's G (or null)
@@ -133,6 +134,8 @@ struct EnumArgs {
     uint32_t gallop_ratio;
     uint32_t use_tma;
     uint32_t failing_sets;
+    uint32_t per_query;             // 1: budget_ns applies to each query from its first task (qstop = 2 on expiry)
+    uint32_t pad;
 };
 
 // ------------------------------------------------------------------ staging
@@ -279,12 +282,15 @@ __device__ __forceinline__ bool query_stopped(const EnumArgs& A, uint32_t q) {
     return __any_sync(kFull, *reinterpret_cast<volatile uint32_t*>(A.qstop + q) != 0);
 }
 
-__device__ void check_global_stop(const EnumArgs& A, uint64_t deadline) {
+// The caller's stop word ends the launch; a passed deadline ends the launch,
+// or with per-query budgets only query q (qstop[q] = 2).
+__device__ void check_global_stop(const EnumArgs& A, uint64_t deadline, uint32_t q = 0) {
     if (lane_id() == 0) {
         int code = 0;
         if (A.host_stop && *A.host_stop) code = SMX_STOPPED;
         else if (deadline && global_timer_ns() > deadline) code = SMX_TIMEOUT;
-        if (code) atomicCAS(A.status, 0, code);
+        if (code == SMX_TIMEOUT && A.per_query) atomicCAS(A.qstop + q, 0u, 2u);
+        else if (code) atomicCAS(A.status, 0, code);
     }
     __syncwarp();
 }
@@ -312,7 +318,7 @@ __device__ __forceinline__ void flush_tally(const EnumArgs& A, Tally& T) {
 // subtree notices them too.
 __device__ __forceinline__ bool task_should_stop(const EnumArgs& A, Tally& T) {
     if (T.local > (1ull << 22)) flush_tally(A, T);
-    if ((++T.polls & 63u) == 0) check_global_stop(A, T.deadline);
+    if ((++T.polls & 63u) == 0) check_global_stop(A, T.deadline, T.q);
     const bool a = poll_abort(A);
     const bool b = query_stopped(A, T.q);
     return a || b;
@@ -835,6 +841,10 @@ __device__ bool lane_should_stop(const EnumArgs& A, uint32_t q, uint64_t deadlin
     int code = 0;
     if (A.host_stop && *A.host_stop) code = SMX_STOPPED;
     else if (deadline && global_timer_ns() > deadline) code = SMX_TIMEOUT;
+    if (code == SMX_TIMEOUT && A.per_query) {
+        atomicCAS(A.qstop + q, 0u, 2u);
+        return true;
+    }
     if (code) {
         atomicCAS(A.status, 0, code);
         return true;
@@ -1326,7 +1336,7 @@ __global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
         for (uint64_t i = lane; i < A.bm_stride; i += 32) bm[i] = 0;
         __syncwarp();
     }
-    const uint64_t deadline = A.budget_ns ? global_timer_ns() + A.budget_ns : 0;
+    const uint64_t deadline = A.budget_ns && !A.per_query ? global_timer_ns() + A.budget_ns : 0;
     Counters C;
     Tally T;
     T.deadline = deadline;
@@ -1363,6 +1373,16 @@ __global__ void __launch_bounds__(256, MINB) enum_kernel(EnumArgs A) {
             const QPlan& P = A.plans[q];
             T.q = q;
             T.local = 0;
+            if (A.per_query) {
+                // the query's budget runs from its first task
+                unsigned long long s0 = 0;
+                if (lane == 0) {
+                    const unsigned long long now = global_timer_ns();
+                    s0 = atomicCAS(A.qstart + q, 0ull, now);
+                    if (s0 == 0) s0 = now;
+                }
+                T.deadline = __shfl_sync(kFull, s0, 0) + A.budget_ns;
+            }
             if (P.mode == SMX_EXPLORE_CANDIDATES) run_table_task(A, P, t - qlo, scr, bm, st, C, T);
             else run_cache_task(A, P, t - qlo, scr, wops, st, C, T);
             flush_tally(A, T);
@@ -1560,7 +1580,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
 int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, const std::vector<const smx_cand*>& cs,
                      const std::vector<const uint32_t*>& orders, const smx_enum_opts& o,
                      const std::vector<uint64_t>& limits, volatile uint32_t* stop, uint64_t* counts, smx_stats* st,
-                     bool use_graph) {
+                     bool use_graph, int32_t* qstatus) {
     SMX_CUDA_TRY(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     const uint32_t nq = (uint32_t)qs.size();
@@ -1643,7 +1663,8 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     const size_t o_qlimit = o_qcount + (size_t)nq * 8;
     const size_t o_prefix = o_qlimit + (size_t)nq * 8;
     const size_t o_qstop = o_prefix + (size_t)(nq + 1) * 8;
-    const size_t o_scr = (o_qstop + (size_t)nq * 4 + 255) & ~(size_t)255;
+    const size_t o_qstart = (o_qstop + (size_t)nq * 4 + 7) & ~(size_t)7;
+    const size_t o_scr = (o_qstart + (size_t)nq * 8 + 255) & ~(size_t)255;
     const size_t o_bm = (o_scr + nwarps * scratch_elems * 4 + 255) & ~(size_t)255;
     const size_t total_bytes = o_bm + nwarps * bm_words * 4 + 64;
     int rc = ensure_scratch(g, total_bytes);
@@ -1656,6 +1677,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     uint64_t* d_qlimit = reinterpret_cast<uint64_t*>(base + o_qlimit);
     uint64_t* d_prefix = reinterpret_cast<uint64_t*>(base + o_prefix);
     uint32_t* d_qstop = reinterpret_cast<uint32_t*>(base + o_qstop);
+    unsigned long long* d_qstart = reinterpret_cast<unsigned long long*>(base + o_qstart);
     uint32_t* d_scr = reinterpret_cast<uint32_t*>(base + o_scr);
     SMX_CUDA_TRY(cudaMemcpyAsync(d_qlimit, limits.data(), nq * 8, cudaMemcpyHostToDevice, s));
     SMX_CUDA_TRY(cudaMemcpyAsync(d_prefix, prefix.data(), (nq + 1) * 8, cudaMemcpyHostToDevice, s));
@@ -1673,6 +1695,8 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     A.next_task = d_next;
     A.qcount = d_qcount;
     A.qstop = d_qstop;
+    A.qstart = d_qstart;
+    A.per_query = (o.budget_per_query && o.time_budget_ms > 0) ? 1u : 0u;
     A.qlimit = d_qlimit;
     A.scratch = d_scr;
     A.stats = d_stats;
@@ -1701,6 +1725,7 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
         if ((e = cudaMemsetAsync(base, 0, 64, ss)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(d_qcount, 0, nq * 8, ss)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(d_qstop, 0, nq * 4, ss)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(d_qstart, 0, nq * 8, ss)) != cudaSuccess) return e;
         SMX_LAUNCH(kern, blocks, wpb * 32, smem, ss, A);
         return cudaGetLastError();
     };
@@ -1730,9 +1755,11 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::vector<unsigned long long> qc(nq);
+    std::vector<uint32_t> qs_stop(nq);
     unsigned long long stats[5];
     int status = 0;
     SMX_CUDA_TRY(cudaMemcpy(qc.data(), d_qcount, nq * 8, cudaMemcpyDeviceToHost));
+    SMX_CUDA_TRY(cudaMemcpy(qs_stop.data(), d_qstop, nq * 4, cudaMemcpyDeviceToHost));
     SMX_CUDA_TRY(cudaMemcpy(stats, d_stats, sizeof(stats), cudaMemcpyDeviceToHost));
     SMX_CUDA_TRY(cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost));
     SMX_CUDA_TRY(cudaFreeAsync(d_pool, s));
@@ -1749,6 +1776,8 @@ int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, cons
         }
         capped += c;
         if (counts) counts[i] = c;
+        if (qstatus) qstatus[i] = qs_stop[i] == 2 ? SMX_TIMEOUT : SMX_OK;
+        if (qs_stop[i] == 2 && status == 0) status = SMX_TIMEOUT;
     }
     if (st) {
         st->count = capped;

@@ -144,7 +144,7 @@ int device_filter(smx_graph* g, const HostQuery& q, int kind, int build_tables, 
 int device_enumerate(smx_graph* g, const std::vector<const HostQuery*>& qs, const std::vector<const smx_cand*>& cs,
                      const std::vector<const uint32_t*>& orders, const smx_enum_opts& o,
                      const std::vector<uint64_t>& limits, volatile uint32_t* stop, uint64_t* counts,
-                     smx_stats* st, bool use_graph);
+                     smx_stats* st, bool use_graph, int32_t* qstatus = nullptr);
 int ensure_scratch(smx_graph* g, size_t bytes);
 // smx_enumerate_noalloc: one query, all working memory in a file-scope device array
 int device_enumerate_noalloc(smx_graph* g, const HostQuery& q, const smx_cand* c, const uint32_t* order,

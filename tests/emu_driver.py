@@ -115,5 +115,5 @@ class Driver:
         counts = np.zeros(nq, dtype=np.uint64)
         st = _lib.StatsC()
         self.check(self.L.smx_enumerate_batch(g, qa, ca, None, nq, ctypes.byref(o), limit, p64(counts),
-                                              ctypes.byref(st)))
+                                              ctypes.byref(st), None))
         return [int(x) for x in counts], st

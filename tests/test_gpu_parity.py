@@ -259,6 +259,27 @@ def test_time_budget_returns_partial_count(gpu, golden):
     assert time.time() - t0 < 30
 
 
+def test_batch_budget_per_query(gpu, golden):
+    """With budget_per_query the budget runs for each query from its first
+    task: the 28.3-billion query stops with SMX_TIMEOUT and a partial count,
+    the small queries of the same launch finish with their exact counts."""
+    hg, dg, _ = device_graph(9500, 35000, 2.5, 1, 1)
+    specs = [(LONG[1], LONG[2], LONG[3]), (4, True, 11), (5, True, 12)]
+    qs, cans = [], []
+    for k, dense, seed in specs:
+        q, _ = query_file(hg, k, dense, seed)
+        can = smx.CandidateParam(dg, q)
+        smx.Filter_GQL(dg, q, can)
+        qs.append(q)
+        cans.append(can)
+    counts, st = smx.explore_batch(dg, qs, cans, opts=smx.EnumOptions(time_budget_ms=20, budget_per_query=1))
+    assert st.status == _lib.SMX_TIMEOUT
+    assert st.query_status == [_lib.SMX_TIMEOUT, 0, 0]
+    assert 0 < counts[0] < golden_count(golden, LONG[0], LONG[1], LONG[3])
+    assert counts[1] == golden_count(golden, "cl9500_unlabelled", 4, 11)
+    assert counts[2] == golden_count(golden, "cl9500_unlabelled", 5, 12)
+
+
 def test_stop_flag_from_another_thread(gpu, golden):
     # a dense 8-vertex query on the 1M-vertex graph runs for minutes uncapped
     hg, dg, _ = device_graph(1_000_000, 10_000_000, 2.2, 1, 2)
