@@ -45,6 +45,8 @@ GAMMA = 2.2
 GRAPH_SEED = 2
 CAP = 1_000_000_000
 WORKLOAD = "cfg2: Chung-Lu 1M V / 10M E (gamma 2.2), 100 queries of 8/12 vertices (half dense), GQL + RI, cap 1e9"
+WORKLOAD3 = ("cfg3: the cfg2 graph with 32 labels drawn Zipf(1.0), queries of 16/24 vertices inheriting labels "
+             "(half dense), NLF + GQL, RI, cache + failing sets, cap 1e9 as a guard")
 METRIC = "queries/s & embeddings/s; learned-order vs RI-order GPU speedup at exact counts"
 
 
@@ -59,18 +61,19 @@ def parse():
     ap.add_argument("--cap", type=int, default=CAP)
     ap.add_argument("--explore", type=int, default=0, help="0 candidate tables, 1 cache + failing sets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", type=int, default=2, choices=[2, 4],
-                    help="2: the headline workload; 4: learned order + batched launch vs RI order one query at a time")
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4],
+                    help="2: the headline workload; 3: its labelled variant; 4: learned order + batched launch vs "
+                         "RI order one query at a time")
     ap.add_argument("--chunk", type=int, default=50, help="--config 4: queries per batched launch")
     ap.add_argument("--train-queries", type=int, default=120, help="--config 4: queries that train the order model")
     return ap.parse_args()
 
 
-def query_specs(nq: int, rank: int):
-    """(k, dense, seed) per query: sizes 8 / 12, dense and sparse alternating."""
+def query_specs(nq: int, rank: int, sizes=(8, 12)):
+    """(k, dense, seed) per query: two sizes, dense and sparse alternating."""
     out = []
     for i in range(nq):
-        k = 8 if (i // 2) % 2 == 0 else 12
+        k = sizes[0] if (i // 2) % 2 == 0 else sizes[1]
         out.append((k, i % 2 == 0, 10_000 + rank * 100_000 + i))
     return out
 
@@ -264,10 +267,13 @@ def run_smx(args, world, rank, local, pg):
 
     torch.cuda.set_device(local)
     dev = local
-    hg = smx.Graph.generate(N_VERT, N_EDGE, GAMMA, 1, 1.0, GRAPH_SEED, device=-1)
+    labelled = args.config == 3
+    hg = smx.Graph.generate(N_VERT, N_EDGE, GAMMA, 32 if labelled else 1, 1.0, GRAPH_SEED, device=-1)
     off, nb, lab = hg.csr()
     dg = smx.Graph.from_csr(off, nb, lab, device=dev)
-    specs = query_specs(args.queries, rank)
+    specs = query_specs(args.queries, rank, sizes=(16, 24) if labelled else (8, 12))
+    if labelled:  # the labelled variant runs the cache + failing-set explorer
+        args.explore = 1
     queries = [smx.Query.generate(hg, k, dense, seed) for k, dense, seed in specs]
     nb_batches = max(1, (len(queries) + args.batch - 1) // args.batch)
     batches = [queries[i * args.batch:(i + 1) * args.batch] for i in range(nb_batches)]
@@ -276,6 +282,7 @@ def run_smx(args, world, rank, local, pg):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
 
     n_enum = [0]
+    at_cap = [0]
 
     def step(graph, batch):
         embeddings = 0
@@ -289,6 +296,7 @@ def run_smx(args, world, rank, local, pg):
                 kernel_ms += st.kernel_ms
                 kbytes += st.bytes
                 n_enum[0] += 1
+                at_cap[0] += bool(st.limit_reached)
         return embeddings, kernel_ms, kbytes
 
     for i in range(args.warmup):
@@ -298,6 +306,7 @@ def run_smx(args, world, rank, local, pg):
     times, emb, kms, kby = [], 0, 0.0, 0
     launches0 = _lib.lib.smx_launch_count()
     n_enum[0] = 0
+    at_cap[0] = 0
     clocks = Clocks(dev)
     clocks.start()
     nq_timed = 0
@@ -320,6 +329,7 @@ def run_smx(args, world, rank, local, pg):
     clock_info = clocks.stop()
     launches = _lib.lib.smx_launch_count() - launches0
     enum_launches = n_enum[0]
+    timed_at_cap = at_cap[0]
     step_ms = max_over_ranks(pg, sum(times) / len(times))
     # ---- e2e: pinned host CSR -> device graph, queries, counts back, per step
     p_off = torch.from_numpy(off.view(np.int64)).pin_memory()
@@ -368,10 +378,12 @@ def run_smx(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded Chung-Lu graph and queries; no dataset download)",
-        "config": {"workload": WORKLOAD, "queries_per_gpu": len(queries), "queries_per_step": args.batch,
+        "config": {"workload": WORKLOAD3 if labelled else WORKLOAD, "queries_per_gpu": len(queries),
+                   "queries_per_step": args.batch,
                    "cap": args.cap,
                    "explore": "candidate tables" if args.explore == 0 else "cache + failing sets",
-                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}",
+                   "timed_queries_at_cap": timed_at_cap},
         "embeddings_per_s": emb * world / (sum(times) / 1000.0),
         "e2e": {"value": q_per_step / (e2e_ms / 1000.0), "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
