@@ -505,35 +505,116 @@ __device__ __forceinline__ uint32_t slot_get(const uint32_t (&a)[2], uint32_t d)
     return __shfl_sync(kFull, d < 32 ? a[0] : a[1], d & 31);
 }
 
+// Slot value of depth d for every lane, each lane naming its own d.
+__device__ __forceinline__ uint32_t slot_get_any(const uint32_t (&a)[2], uint32_t d) {
+    const uint32_t lo = __shfl_sync(kFull, a[0], d & 31);
+    const uint32_t hi = __shfl_sync(kFull, a[1], d & 31);
+    return d < 32 ? lo : hi;
+}
+
 // Computes the partial intersections that end at depth d (its candidate just
 // chosen).  Returns false as soon as one is empty: no embedding extends the
-// candidate.
+// candidate.  Lane p describes part p.  Parts whose lists are both long go
+// through the staged merge one at a time; the galloping ones (short list
+// against a long row) run together, one lane per element of their short
+// lists, so their binary searches overlap instead of following each other.
 __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& st, uint32_t gallop_ratio,
                               Counters& C, const uint32_t (&slot_idx)[2]) {
     const DepthInfo& D = P.dep[d];
-    for (uint32_t i = 0; i < D.npart; ++i) {
-        const PartRef R = P.part[D.part_begin + i];
-        Row a;
-        if (R.prev_off == kInvalid) {
-            const BnRef B = P.bn[R.bn_first];
-            a = table_row(B, slot_get(slot_idx, B.depth));
-        } else {
-            a = part_list(scr, R.prev_off);
+    const uint32_t lane = lane_id();
+    for (uint32_t base = 0; base < D.npart; base += 32) {
+        const bool has = lane < D.npart - base;
+        PartRef R{0, 0, kInvalid, 0};
+        BnRef Bf{}, Bt{};
+        if (has) {
+            R = P.part[D.part_begin + base + lane];
+            Bt = P.bn[R.bn_this];
+            if (R.prev_off == kInvalid) Bf = P.bn[R.bn_first];
         }
-        const BnRef B2 = P.bn[R.bn_this];
-        const Row b = table_row(B2, slot_get(slot_idx, B2.depth));
-        uint32_t* out = scr + R.out_off;
-        uint32_t k = 0;
-        if (a.len && b.len) {
-            C.isect++;
-            C.bytes += 4ull * (a.len + b.len) + 8;
-            k = a.len <= b.len ? isect<false>(st, gallop_ratio, a.p, a.len, b.p, b.len, out + 4)
-                               : isect<false>(st, gallop_ratio, b.p, b.len, a.p, a.len, out + 4);
+        const uint32_t i_this = slot_get_any(slot_idx, has ? Bt.depth : 0);
+        const uint32_t i_first = slot_get_any(slot_idx, has && R.prev_off == kInvalid ? Bf.depth : 0);
+        Row a{nullptr, 0}, b{nullptr, 0};
+        uint32_t* out = nullptr;
+        if (has) {
+            a = R.prev_off == kInvalid ? table_row(Bf, i_first) : part_list(scr, R.prev_off);
+            b = table_row(Bt, i_this);
+            if (a.len > b.len) {
+                const Row t = a;
+                a = b;
+                b = t;
+            }
+            out = scr + R.out_off;
+        }
+        if (__any_sync(kFull, has && a.len == 0)) return false;
+        C.isect += __popc(__ballot_sync(kFull, has));
+        C.bytes += __reduce_add_sync(kFull, has ? 4u * (a.len + b.len) + 8u : 0u);
+        const bool gal = has && (uint64_t)a.len * gallop_ratio < b.len;
+        // long against long: staged merge, one part at a time
+        uint32_t mm = __ballot_sync(kFull, has && !gal);
+        while (mm) {
+            const int p = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const uint32_t* pa = reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(a.p), p));
+            const uint32_t* pb = reinterpret_cast<const uint32_t*>(shfl64(reinterpret_cast<uint64_t>(b.p), p));
+            uint32_t* po = reinterpret_cast<uint32_t*>(shfl64(reinterpret_cast<uint64_t>(out), p));
+            const uint32_t la = __shfl_sync(kFull, a.len, p), lb = __shfl_sync(kFull, b.len, p);
+            const uint32_t k = isect<false>(st, gallop_ratio, pa, la, pb, lb, po + 4);
+            __syncwarp();
+            if (lane == 0) po[0] = k;
+            __syncwarp();
+            if (k == 0) return false;
+        }
+        // short against long: all galloping parts in one pass
+        const uint32_t gm = __ballot_sync(kFull, gal);
+        if (!gm) continue;
+        const uint32_t len_g = gal ? a.len : 0;
+        uint32_t incl = len_g;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t excl = incl - len_g;
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        uint32_t found = 0;  // lane p: elements of part p kept so far
+        for (uint32_t g0 = 0; g0 < total; g0 += 32) {
+            const uint32_t gi = g0 + lane;
+            uint32_t mp = 32, off = 0, mbl = 0;
+            const uint32_t* ma = nullptr;
+            const uint32_t* mb = nullptr;
+            for (uint32_t m = gm; m; m &= m - 1) {
+                const int q = __ffs(m) - 1;
+                const uint32_t ex = __shfl_sync(kFull, excl, q), ln = __shfl_sync(kFull, len_g, q);
+                const uint64_t ap = shfl64(reinterpret_cast<uint64_t>(a.p), q);
+                const uint64_t bp = shfl64(reinterpret_cast<uint64_t>(b.p), q);
+                const uint32_t bl = __shfl_sync(kFull, b.len, q);
+                if (gi < total && gi >= ex && gi < ex + ln) {
+                    mp = (uint32_t)q;
+                    off = gi - ex;
+                    ma = reinterpret_cast<const uint32_t*>(ap);
+                    mb = reinterpret_cast<const uint32_t*>(bp);
+                    mbl = bl;
+                }
+            }
+            uint32_t x = 0;
+            bool hit = false;
+            if (mp < 32) {
+                x = ma[off];
+                hit = bsearch_global(mb, mbl, x);
+            }
+            for (uint32_t m = gm; m; m &= m - 1) {
+                const int q = __ffs(m) - 1;
+                const uint32_t hm = __ballot_sync(kFull, hit && mp == (uint32_t)q);
+                if (!hm) continue;
+                const uint32_t before = __shfl_sync(kFull, found, q);
+                uint32_t* oq = reinterpret_cast<uint32_t*>(shfl64(reinterpret_cast<uint64_t>(out), q));
+                if (hit && mp == (uint32_t)q) oq[4 + before + __popc(hm & lanemask_lt())] = x;
+                if (lane == (uint32_t)q) found += __popc(hm);
+            }
         }
         __syncwarp();
-        if (lane_id() == 0) out[0] = k;
+        if (gal) out[0] = found;
         __syncwarp();
-        if (k == 0) return false;
+        if (__any_sync(kFull, gal && found == 0)) return false;
     }
     return true;
 }

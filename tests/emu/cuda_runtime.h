@@ -251,6 +251,14 @@ inline unsigned __reduce_or_sync(unsigned, unsigned v) {
     emu::wsync();
     return r;
 }
+inline unsigned __reduce_add_sync(unsigned, unsigned v) {
+    emu::slots()[emu::ctx.lane] = v;
+    emu::wsync();
+    unsigned r = 0;
+    for (unsigned i = 0; i < 32; ++i) r += (unsigned)emu::slots()[i];
+    emu::wsync();
+    return r;
+}
 inline unsigned __reduce_min_sync(unsigned, unsigned v) {
     emu::slots()[emu::ctx.lane] = v;
     emu::wsync();
