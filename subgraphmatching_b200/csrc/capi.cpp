@@ -199,6 +199,8 @@ void smx_graph_destroy(smx_graph* g) {
     cudaFree(g->d_adj);
     cudaFree(g->d_lab);
     cudaFree(g->d_hist);
+    cudaFree(g->d_hub_id);
+    cudaFree(g->d_hub_bits);
     cudaFree(g->d_scratch);
     for (auto& e : g->mark)
         if (e) cudaEventDestroy(e);

@@ -75,6 +75,18 @@ __device__ __forceinline__ bool bsearch_shared(const uint32_t* a, uint32_t n, ui
     return a[base] == x;
 }
 
+// Branch-free search in read-only memory (data graph rows, tables).
+__device__ __forceinline__ bool bsearch_ldg(const uint32_t* a, uint32_t n, uint32_t x) {
+    if (n == 0) return false;
+    uint32_t base = 0;
+    while (n > 1) {
+        uint32_t half = n >> 1;
+        base = (__ldg(a + base + half) <= x) ? base + half : base;
+        n -= half;
+    }
+    return __ldg(a + base) == x;
+}
+
 // Number of elements <= x in sorted a[0, n) (global memory, coherent loads).
 __device__ __forceinline__ uint32_t upper_bound_global(const uint32_t* a, uint32_t n, uint32_t x) {
     uint32_t lo = 0, hi = n;

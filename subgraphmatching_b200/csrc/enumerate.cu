@@ -75,6 +75,7 @@ struct PartRef {
     uint32_t bn_this;   // BnRef of p_j
     uint32_t prev_off;  // buffer of P_t^{j-1}; kInvalid when j == 2
     uint32_t out_off;   // buffer of P_t^j
+    uint32_t target;    // t
 };
 
 struct OpInfo {
@@ -106,7 +107,9 @@ struct QPlan {
     uint32_t leaf_g_off;   // kInvalid unless G is a partial buffer
     uint32_t leaf_gp_off;  // buffer for G without the embedded vertices
     uint32_t leaf_bm;      // 1: G may be marked in the warp's bitmap (indices into C(u_L))
-    uint32_t pad2;
+    uint32_t hub_words;    // words per row of the hub adjacency matrix (0: none)
+    const uint32_t* hub_id;
+    const uint32_t* hub_bits;
     DepthInfo dep[kMaxQ];
 };
 
@@ -335,6 +338,16 @@ __device__ __forceinline__ Row table_row(const BnRef& r, uint32_t idx) {
     return Row{r.edge + s, __ldg(r.off + idx + 1) - s};
 }
 
+// Data vertices v (hub id hv, or kInvalid) and w adjacent?  Two hubs: one
+// bit of the hub matrix; otherwise a binary search of the shorter row.
+__device__ __forceinline__ bool adjacent(const QPlan& P, uint32_t v, uint32_t hv, uint32_t w, uint32_t hw) {
+    if (hv != kInvalid && hw != kInvalid)
+        return (__ldg(P.hub_bits + (size_t)hv * P.hub_words + (hw >> 5)) >> (hw & 31)) & 1u;
+    const uint64_t ov = __ldg(P.off + v), ow = __ldg(P.off + w);
+    const uint32_t dv = (uint32_t)(__ldg(P.off + v + 1) - ov), dw = (uint32_t)(__ldg(P.off + w + 1) - ow);
+    return dv <= dw ? bsearch_ldg(P.adj + ov, dv, w) : bsearch_ldg(P.adj + ow, dw, v);
+}
+
 // Candidate list of depth D (CandidatesBuffer::getNextCandidatesImpl,
 // explore.h:284-354): with one backward neighbour the table row itself (no
 // copy), otherwise the intersection of all rows, shortest first, in the
@@ -519,9 +532,13 @@ __device__ __forceinline__ uint32_t slot_get_any(const uint32_t (&a)[2], uint32_
 // against a long row) run together, one lane per element of their short
 // lists, so their binary searches overlap instead of following each other.
 __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& st, uint32_t gallop_ratio,
-                              Counters& C, const uint32_t (&slot_idx)[2]) {
+                              Counters& C, const uint32_t (&slot_idx)[2], const uint32_t (&slot_vid)[2]) {
     const DepthInfo& D = P.dep[d];
     const uint32_t lane = lane_id();
+    // the vertex just chosen at depth d: galloping against its rows can test
+    // adjacency directly (hub matrix) instead of searching the row
+    const uint32_t vd = slot_get_any(slot_vid, d);
+    const uint32_t hvd = (D.npart && P.hub_words) ? __ldg(P.hub_id + vd) : kInvalid;
     for (uint32_t base = 0; base < D.npart; base += 32) {
         const bool has = lane < D.npart - base;
         PartRef R{0, 0, kInvalid, 0};
@@ -535,6 +552,7 @@ __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& 
         const uint32_t i_first = slot_get_any(slot_idx, has && R.prev_off == kInvalid ? Bf.depth : 0);
         Row a{nullptr, 0}, b{nullptr, 0};
         uint32_t* out = nullptr;
+        const uint32_t* tcand = nullptr;  // C(u_t) when b is depth d's row (adjacency test possible)
         if (has) {
             a = R.prev_off == kInvalid ? table_row(Bf, i_first) : part_list(scr, R.prev_off);
             b = table_row(Bt, i_this);
@@ -542,6 +560,8 @@ __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& 
                 const Row t = a;
                 a = b;
                 b = t;
+            } else if (hvd != kInvalid) {
+                tcand = P.dep[R.target].cand;
             }
             out = scr + R.out_off;
         }
@@ -581,17 +601,20 @@ __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& 
             uint32_t mp = 32, off = 0, mbl = 0;
             const uint32_t* ma = nullptr;
             const uint32_t* mb = nullptr;
+            const uint32_t* mc = nullptr;
             for (uint32_t m = gm; m; m &= m - 1) {
                 const int q = __ffs(m) - 1;
                 const uint32_t ex = __shfl_sync(kFull, excl, q), ln = __shfl_sync(kFull, len_g, q);
                 const uint64_t ap = shfl64(reinterpret_cast<uint64_t>(a.p), q);
                 const uint64_t bp = shfl64(reinterpret_cast<uint64_t>(b.p), q);
+                const uint64_t cp = shfl64(reinterpret_cast<uint64_t>(tcand), q);
                 const uint32_t bl = __shfl_sync(kFull, b.len, q);
                 if (gi < total && gi >= ex && gi < ex + ln) {
                     mp = (uint32_t)q;
                     off = gi - ex;
                     ma = reinterpret_cast<const uint32_t*>(ap);
                     mb = reinterpret_cast<const uint32_t*>(bp);
+                    mc = reinterpret_cast<const uint32_t*>(cp);
                     mbl = bl;
                 }
             }
@@ -599,7 +622,13 @@ __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& 
             bool hit = false;
             if (mp < 32) {
                 x = ma[off];
-                hit = bsearch_global(mb, mbl, x);
+                if (mc) {
+                    // x in row(v_d) <=> C(u_t)[x] adjacent to v_d
+                    const uint32_t w = __ldg(mc + x);
+                    hit = adjacent(P, vd, hvd, w, __ldg(P.hub_id + w));
+                } else {
+                    hit = bsearch_global(mb, mbl, x);
+                }
             }
             for (uint32_t m = gm; m; m &= m - 1) {
                 const int q = __ffs(m) - 1;
@@ -641,6 +670,7 @@ struct LeafState {
     uint32_t prank0, prank1;
     uint64_t pmask;    // depths with a valid prank
     uint32_t* bm;      // the warp bitmap while G is marked in it, else null
+    uint32_t hub;      // 1: G's vertex ids and hub ids are staged after G (shared memory, words 256 / 512)
 };
 
 // Per-lane |row ∩ G| by probing G's membership bitmap: one independent load
@@ -710,6 +740,7 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uin
     }
     S.pmask = pm;
     S.k0 = S.glen - __popcll(pm);
+    S.hub = 0;
     if (S.inb && S.gany) {
         // G minus the embedded vertices, into shared memory when it fits (the
         // stage buffer is idle until depth n-2 is left), else into its buffer;
@@ -742,6 +773,18 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uin
         S.glen = k;
         S.pmask = 0;
         S.k0 = k;
+        S.hub = 0;
+        if (in_smem && k <= 256 && st.chunk >= 768 && P.hub_words) {
+            // G's data vertices and their hub ids, for adjacency tests per lane
+            const uint32_t* candL = D.cand;
+            for (uint32_t i = lane; i < k; i += 32) {
+                const uint32_t w = __ldg(candL + dst[i]);
+                st.buf[256 + i] = w;
+                st.buf[512 + i] = __ldg(P.hub_id + w);
+            }
+            __syncwarp();
+            S.hub = 1;
+        }
         if (bm && P.leaf_bm && k >= bitmap_min) {
             for (uint32_t i = lane; i < k; i += 32) atomicOr(bm + (dst[i] >> 5), 1u << (dst[i] & 31));
             __syncwarp();
@@ -754,7 +797,7 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uin
 // batch at once, one candidate per lane.  Adds the algorithmic bytes of the
 // whole warp to C.bytes.
 __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_t* lp, uint32_t base, uint32_t vm,
-                               Counters& C) {
+                               Counters& C, const uint32_t* st_buf) {
     const uint32_t lane = lane_id();
     const uint32_t L = P.n - 1;
     const uint32_t u = P.dep[L].u;
@@ -776,7 +819,22 @@ __device__ uint64_t leaf_batch(const QPlan& P, const LeafState& S, const uint32_
             const Row r = table_row(S.row, c);
             row = r.p;
             row_len = r.len;
-            if (S.bm && r.len <= S.glen * (32u - __clz(r.len))) {
+            uint32_t vc = 0, hc = kInvalid;
+            if (S.hub) {
+                vc = __ldg(P.dep[L - 1].cand + c);
+                hc = __ldg(P.hub_id + vc);
+            }
+            if (hc != kInvalid && r.len > S.glen) {
+                // a hub candidate: test each vertex of G against it (the hub
+                // matrix for hub pairs, independent loads) instead of
+                // searching its long row
+                const uint32_t* gv = st_buf + 256;
+                const uint32_t* gh = st_buf + 512;
+                uint32_t k = 0;
+                for (uint32_t i = 0; i < S.glen; ++i) k += adjacent(P, vc, hc, gv[i], gh[i]);
+                cnt = k;
+                bytes = 12 + 4 * S.glen;
+            } else if (S.bm && r.len <= S.glen * (32u - __clz(r.len))) {
                 // probes of the bitmap (independent loads) cost less than
                 // |G| searches of the row (dependent loads)
                 cnt = lane_count_bitmap(r.p, r.len, S.bm);
@@ -1045,7 +1103,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
 #define vid0 slot_vid[0]
 #define vid1 slot_vid[1]
     // partials ending at depth 1 (depth 0 is every target's first backward neighbour)
-    if (!compute_parts(P, 1, scr, st, A.gallop_ratio, C, slot_idx)) return;
+    if (!compute_parts(P, 1, scr, st, A.gallop_ratio, C, slot_idx, slot_vid)) return;
     uint32_t d = 2;
     LeafState leaf;
     leaf.bm = nullptr;
@@ -1128,7 +1186,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
             // all valid candidates of this batch at once, one per lane
             const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
             const uint32_t base = SLOT_GET(pos, d) - 32;
-            local += leaf_batch(P, leaf, lp, base, vm, C);
+            local += leaf_batch(P, leaf, lp, base, vm, C, st.buf);
             C.nodes += __popc(vm);
             SLOT_SET(vm, d, 0u);
             continue;
@@ -1142,7 +1200,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(idx, d, c);
         SLOT_SET(vid, d, v);
         C.nodes++;
-        if (!compute_parts(P, d, scr, st, A.gallop_ratio, C, slot_idx)) continue;
+        if (!compute_parts(P, d, scr, st, A.gallop_ratio, C, slot_idx, slot_vid)) continue;
         ++d;
         open_depth(d);
     }
@@ -1506,6 +1564,9 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
     P.mask = c->d_mask;
     P.off = g->d_off;
     P.adj = g->d_adj;
+    P.hub_id = g->d_hub_id;
+    P.hub_bits = g->d_hub_bits;
+    P.hub_words = g->hubs ? g->hub_words : 0;
     P.nroot = c->cnt[order[0]];
     std::vector<uint32_t> depth_of(n);
     for (uint32_t i = 0; i < n; ++i) depth_of[order[i]] = i;
@@ -1576,7 +1637,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                 const uint32_t e = D.bn_begin + j - 1;
                 cap = std::min<uint64_t>(cap, hb.bn[e].max_deg);
                 const uint32_t off = alloc(cap);
-                parts_at[hb.bn[e].depth].push_back(PartRef{D.bn_begin, e, prev, off});
+                parts_at[hb.bn[e].depth].push_back(PartRef{D.bn_begin, e, prev, off, t});
                 prev = off;
             }
             if (!leaf) {

@@ -15,6 +15,7 @@
 //                         indices into C(b) (edge_v is C(b)[edge], rebuilt on
 //                         export), ascending rows, as buildTables (table.h:7-139)
 #include <algorithm>
+#include <numeric>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -622,6 +623,35 @@ int upload_graph(smx_graph* g) {
         SMX_LAUNCH(hist_kernel, grid_for(g, h.n, 256), 256, 0, st, g->d_off, g->d_adj, g->d_lab, h.n, g->hist_stride,
                    g->d_hist);
         SMX_CUDA_TRY(cudaGetLastError());
+    }
+    {
+        // hub adjacency (used by the enumerator for membership tests)
+        constexpr uint32_t kMaxHubs = 16384, kMinHubDeg = 16;
+        std::vector<uint32_t> byd(h.n);
+        std::iota(byd.begin(), byd.end(), 0u);
+        const uint32_t k = std::min<uint32_t>(kMaxHubs, h.n);
+        std::partial_sort(byd.begin(), byd.begin() + k, byd.end(), [&](uint32_t a, uint32_t b) {
+            return h.deg(a) != h.deg(b) ? h.deg(a) > h.deg(b) : a < b;
+        });
+        uint32_t hubs = 0;
+        while (hubs < k && h.deg(byd[hubs]) >= kMinHubDeg) ++hubs;
+        g->hubs = hubs;
+        g->hub_words = (hubs + 31) / 32;
+        std::vector<uint32_t> hid(h.n, 0xffffffffu);
+        for (uint32_t i = 0; i < hubs; ++i) hid[byd[i]] = i;
+        std::vector<uint32_t> bits((size_t)hubs * g->hub_words, 0u);
+        for (uint32_t i = 0; i < hubs; ++i) {
+            const uint32_t v = byd[i];
+            for (uint64_t e = h.off[v]; e < h.off[v + 1]; ++e) {
+                const uint32_t j = hid[h.adj[e]];
+                if (j != 0xffffffffu) bits[(size_t)i * g->hub_words + (j >> 5)] |= 1u << (j & 31);
+            }
+        }
+        SMX_CUDA_TRY(cudaMalloc(&g->d_hub_id, (size_t)std::max<uint32_t>(h.n, 1) * 4));
+        SMX_CUDA_TRY(cudaMalloc(&g->d_hub_bits, std::max<size_t>(bits.size(), 1) * 4));
+        if (h.n) SMX_CUDA_TRY(cudaMemcpyAsync(g->d_hub_id, hid.data(), (size_t)h.n * 4, cudaMemcpyHostToDevice, st));
+        if (!bits.empty())
+            SMX_CUDA_TRY(cudaMemcpyAsync(g->d_hub_bits, bits.data(), bits.size() * 4, cudaMemcpyHostToDevice, st));
     }
     SMX_CUDA_TRY(cudaStreamSynchronize(st));
     return SMX_OK;

@@ -104,6 +104,12 @@ struct smx_graph {
     uint32_t* d_lab = nullptr;   // n
     uint8_t* d_hist = nullptr;   // n * hist_stride neighbour-label counts (saturating), labelled graphs only
     uint32_t hist_stride = 0;
+    // hub adjacency: the (up to) 16,384 highest-degree vertices (degree >= 16)
+    // get ids; bit (i, j) of a hub_words-per-row matrix says hubs i and j
+    // are adjacent (32 MB at most, kept in L2 by the enumerator's probes)
+    uint32_t* d_hub_id = nullptr;    // n: hub id or 0xffffffff
+    uint32_t* d_hub_bits = nullptr;  // hubs * hub_words
+    uint32_t hubs = 0, hub_words = 0;
     // scratch reused across calls
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
