@@ -110,6 +110,12 @@ struct QPlan {
     uint32_t hub_words;    // words per row of the hub adjacency matrix (0: none)
     const uint32_t* hub_id;
     const uint32_t* hub_bits;
+    // factored tail (candidate-table mode): the lists S of depth n-2 and G of
+    // the last depth (without depth n-2's row) depend only on depths <=
+    // tail_depth (kInvalid: not used); tail_rev = E[u_L][u_{n-2}]
+    uint32_t tail_depth;
+    uint32_t tail_bms;     // word offset of S's bitmap after G's in the warp bitmap
+    BnRef tail_rev;
     DepthInfo dep[kMaxQ];
 };
 
@@ -1061,6 +1067,112 @@ __device__ uint64_t lane_subtree(const EnumArgs& A, const QPlan& P, uint32_t d0,
     return cnt;
 }
 
+// ------------------------------------------------------------------ factored tail
+// When S (the list of depth n-2) and G (the last depth's list without the
+// row of depth n-2) depend only on depths <= a < n-3, the count below a
+// depth-(n-3) node is
+//   sum over c in S \ E, g in G \ E of [c ~ g]
+// with E the vertices embedded at depths 0 .. n-3.  By inclusion-exclusion
+//   = B - sum_{e in E ∩ S} |N(e) ∩ G| - sum_{e in E ∩ G} |N(e) ∩ S|
+//       + #{(e, f) in (E ∩ S) x (E ∩ G) : e ~ f}
+// where B = sum_{c in S} |N(c) ∩ G| is computed once per depth-a node.  S and
+// G stay marked in the warp's bitmaps (over C(u_{n-2}) and C(u_L) indices)
+// while they are valid.
+
+__device__ __forceinline__ Row tail_list(const QPlan& P, uint32_t* scr, uint32_t off, uint32_t bn,
+                                         const uint32_t (&slot_idx)[2]) {
+    if (off != kInvalid) return part_list(scr, off);
+    const BnRef R = P.bn[bn];
+    return table_row(R, slot_get(slot_idx, R.depth));
+}
+
+__device__ void tail_mark(Row X, uint32_t* bmx, bool set) {
+    __syncwarp();
+    for (uint32_t i = lane_id(); i < X.len; i += 32) {
+        const uint32_t x = X.p[i];
+        if (set) atomicOr(bmx + (x >> 5), 1u << (x & 31));
+        else atomicAnd(bmx + (x >> 5), ~(1u << (x & 31)));
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ bool bm_test(const uint32_t* bmx, uint32_t x) {
+    return (__ldcg(bmx + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// B = sum over c in S of |row_{n-2 -> L}(c) ∩ G| (G marked in bmG)
+__device__ uint64_t tail_base(Row S, const BnRef& rowSL, const uint32_t* bmG, Counters& C) {
+    uint64_t sum = 0;
+    uint32_t bytes = 0;
+    for (uint32_t base = 0; base < S.len; base += 32) {
+        const uint32_t i = base + lane_id();
+        if (i < S.len) {
+            const Row r = table_row(rowSL, S.p[i]);
+            sum += lane_count_bitmap(r.p, r.len, bmG);
+            bytes += 8 * r.len;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        sum += __shfl_xor_sync(kFull, sum, o);
+        bytes += __shfl_xor_sync(kFull, bytes, o);
+    }
+    C.bytes += bytes;
+    return sum;
+}
+
+// B - the corrections for E = the vertices at depths 0 .. n-3
+__device__ uint64_t tail_count(const QPlan& P, uint64_t base, const uint32_t (&slot_vid)[2], const BnRef& rowSL,
+                               const uint32_t* bmS, const uint32_t* bmG) {
+    const uint32_t lane = lane_id();
+    const uint32_t nE = P.n - 2;
+    const uint32_t uS = P.dep[P.n - 2].u, uL = P.dep[P.n - 1].u;
+    uint32_t e[2], he[2];
+    bool inS[2], inG[2];
+    uint64_t t12 = 0;
+    for (uint32_t h = 0; h < 2; ++h) {
+        const uint32_t j = h * 32 + lane;
+        e[h] = kInvalid;
+        he[h] = kInvalid;
+        inS[h] = inG[h] = false;
+        if (j < nE) {
+            e[h] = slot_vid[h];
+            const uint64_t m = __ldg(P.mask + e[h]);
+            if ((m >> uS) & 1ull) {
+                const uint32_t rS = cand_rank(P.rank, P.qn, uS, e[h]);
+                if (bm_test(bmS, rS)) {
+                    inS[h] = true;
+                    const Row r = table_row(rowSL, rS);
+                    t12 += lane_count_bitmap(r.p, r.len, bmG);
+                }
+            }
+            if ((m >> uL) & 1ull) {
+                const uint32_t rG = cand_rank(P.rank, P.qn, uL, e[h]);
+                if (bm_test(bmG, rG)) {
+                    inG[h] = true;
+                    const Row r = table_row(P.tail_rev, rG);
+                    t12 += lane_count_bitmap(r.p, r.len, bmS);
+                }
+            }
+            if (P.hub_words) he[h] = __ldg(P.hub_id + e[h]);
+        }
+    }
+    // pairs (e in S, f in G) of embedded vertices that are adjacent
+    uint64_t t3 = 0;
+    for (uint32_t hf = 0; hf < 2; ++hf) {
+        for (uint32_t gm = __ballot_sync(kFull, inG[hf]); gm; gm &= gm - 1) {
+            const int q = __ffs(gm) - 1;
+            const uint32_t f = __shfl_sync(kFull, e[hf], q), hfid = __shfl_sync(kFull, he[hf], q);
+            for (uint32_t h = 0; h < 2; ++h)
+                if (inS[h] && e[h] != f) t3 += adjacent(P, e[h], he[h], f, hfid);
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        t12 += __shfl_xor_sync(kFull, t12, o);
+        t3 += __shfl_xor_sync(kFull, t3, o);
+    }
+    return base - t12 + t3;
+}
+
 // One task: root r = row of entry t in E[o0][o1], depth-1 candidate edge[t].
 __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, uint32_t* scr, uint32_t* bm, Stage& st,
                                Counters& C, Tally& T) {
@@ -1107,6 +1219,26 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
     uint32_t d = 2;
     LeafState leaf;
     leaf.bm = nullptr;
+    // factored tail: S and G marked in the bitmaps and B valid for the current prefix
+    const bool tail = P.tail_depth != kInvalid && bm != nullptr;
+    bool tail_live = false;
+    uint64_t tail_b = 0;
+    const DepthInfo& DL = P.dep[n - 1];
+    const BnRef rowSL = P.bn[DL.bn_begin + DL.nbn - 1];
+    uint32_t* bmG = bm;
+    uint32_t* bmS = bm ? bm + P.tail_bms : nullptr;
+    auto tail_lists = [&](Row& S, Row& G) {
+        S = tail_list(P, scr, P.dep[n - 2].list_off, P.dep[n - 2].bn_begin, slot_idx);
+        G = tail_list(P, scr, P.leaf_g_off, P.leaf_g_bn, slot_idx);
+    };
+    auto tail_drop = [&]() {
+        if (!tail_live) return;
+        Row S, G;
+        tail_lists(S, G);
+        tail_mark(S, bmS, false);
+        tail_mark(G, bmG, false);
+        tail_live = false;
+    };
     auto open_depth = [&](uint32_t dd) {
         const DepthInfo& D = P.dep[dd];
         Row r;
@@ -1120,6 +1252,21 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         SLOT_SET(len, dd, r.len);
         SLOT_SET(pos, dd, 0u);
         SLOT_SET(vm, dd, 0u);
+        if (tail && dd + 2 == n) {
+            // the whole subtree below this depth-(n-3) node, counted at once
+            if (!tail_live) {
+                Row S, G;
+                tail_lists(S, G);
+                tail_mark(S, bmS, true);
+                tail_mark(G, bmG, true);
+                tail_b = tail_base(S, rowSL, bmG, C);
+                tail_live = true;
+            }
+            local += tail_count(P, tail_b, slot_vid, rowSL, bmS, bmG);
+            C.nodes += r.len;
+            SLOT_SET(len, dd, 0u);
+            return;
+        }
         if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf, bm, A.bitmap_min);
     };
     open_depth(2);
@@ -1197,6 +1344,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         const uint32_t* lp = reinterpret_cast<const uint32_t*>(shfl64(d < 32 ? ptr0 : ptr1, d & 31));
         const uint32_t c = lp[pos];
         const uint32_t v = __ldg(P.dep[d].cand + c);
+        if (tail && d <= P.tail_depth) tail_drop();  // S and G change with this depth
         SLOT_SET(idx, d, c);
         SLOT_SET(vid, d, v);
         C.nodes++;
@@ -1205,6 +1353,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         open_depth(d);
     }
     leaf_clear(leaf);  // a stop can leave depth n-2 early
+    tail_drop();
 #undef idx0
 #undef idx1
 #undef vid0
@@ -1615,6 +1764,8 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
     }
     P.leaf_inb = 0;
     P.leaf_bm = 0;
+    P.tail_depth = kInvalid;
+    P.tail_bms = 0;
     P.leaf_g_bn = P.leaf_g_off = P.leaf_gp_off = kInvalid;
     if (mode == SMX_EXPLORE_CANDIDATES) {
         // partial-intersection buffers: word 0 the length, elements from word 4
@@ -1651,6 +1802,22 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                     if (use_bitmap) {
                         P.leaf_bm = 1;
                         hb.bm_words = (uint64_t)c->cnt[order[t]] / 32 + 1;
+                        // factored tail: S and G depend only on depths <= a, with
+                        // a at least one depth above n-3
+                        uint32_t a = 0;
+                        for (uint32_t p : bnd[n - 2]) a = std::max(a, p);
+                        for (uint32_t j = 0; j < jmax; ++j) a = std::max(a, bnd[t][j]);
+                        const int ti = c->tab_index[order[t]][order[n - 2]];
+                        if (n >= 5 && a + 4 <= n && ti >= 0) {
+                            P.tail_depth = a;
+                            P.tail_bms = (uint32_t)hb.bm_words;
+                            hb.bm_words += (uint64_t)c->cnt[order[n - 2]] / 32 + 1;
+                            const DevTable& T = c->tables[ti];
+                            P.tail_rev.off = T.d_off;
+                            P.tail_rev.edge = T.d_edge;
+                            P.tail_rev.depth = t;
+                            P.tail_rev.max_deg = T.max_deg;
+                        }
                     }
                 }
             }
