@@ -5,11 +5,25 @@ this catches warp-logic errors (divergent shuffles, slot bookkeeping,
 failing-set pruning) before a GPU run."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
 from emu_driver import p32
-from helpers import host_graph, query_file
+from helpers import TMP, host_graph, query_file
+
+
+def smx_generate(n, m, seed):
+    import subgraphmatching_b200 as smx
+
+    return smx.Graph.generate(n, m, 2.2, 1, 1.0, seed=seed, device=-1)
+
+
+def smx_query(g, k, seed):
+    import subgraphmatching_b200 as smx
+
+    return smx.Query.generate(g, k, dense=True, seed=seed)
 
 CASES = [  # (n, m, labels, seed, [(k, dense, qseed)], filter kinds)
     (300, 900, 1, 5, [(4, True, 2), (5, False, 3)], (1,)),
@@ -128,3 +142,30 @@ def test_emulated_graph_destroyed_before_its_candidates(emu):
     assert emu.L.smx_cand_export(c, 0, p32(np.zeros(8, dtype=np.uint32))) == 6  # SMX_BAD_ARGUMENT
     emu.L.smx_cand_destroy(c)
     emu.L.smx_query_destroy(dq)
+
+
+def test_emulated_factored_tail(emu, port):
+    """Queries whose last two depths close on shallow vertices (the factored
+    tail: one sum per shallow node, corrected per node by inclusion-exclusion
+    over the embedded vertices) against the oracle, with the tail on (default)
+    and off (bitmap_min = -1)."""
+    g = smx_generate(600, 2400, 7)
+    off, nb, lab = g.csr()
+    dg = emu.graph(off, nb, lab)
+    path = os.path.join(TMP, "g600_2400_7.txt")
+    g.save(path)
+    gp = port.load_graph(path)
+    for k, seed in [(8, 1055), (7, 1110), (6, 1157)]:
+        q = smx_query(g, k, seed)
+        qpath = os.path.join(TMP, f"tail_q{seed}.txt")
+        q.save(qpath)
+        qp = port.load_query(qpath)
+        qo, qn, ql = q.csr()
+        dq = emu.query(qo, qn, ql)
+        c, ok = emu.filter(dg, dq, 1)
+        assert ok
+        order = emu.order_ri(dq, k)
+        ref = min(port.explore(gp, qp, port.filter(gp, qp, 1), order, 3_000_000, 8)[0], 3_000_000)
+        assert ref > 0
+        for bmin in (0, -1):
+            assert emu.enumerate(dg, dq, c, order, explore=0, limit=3_000_000, bitmap_min=bmin).count == ref
