@@ -1802,13 +1802,14 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                     if (use_bitmap) {
                         P.leaf_bm = 1;
                         hb.bm_words = (uint64_t)c->cnt[order[t]] / 32 + 1;
-                        // factored tail: S and G depend only on depths <= a, with
-                        // a at least one depth above n-3
+                        // factored tail: S and G depend only on depths <= a; B is
+                        // recomputed per depth-a node, so it pays only with at
+                        // least three depths between a and n-2
                         uint32_t a = 0;
                         for (uint32_t p : bnd[n - 2]) a = std::max(a, p);
                         for (uint32_t j = 0; j < jmax; ++j) a = std::max(a, bnd[t][j]);
                         const int ti = c->tab_index[order[t]][order[n - 2]];
-                        if (n >= 5 && a + 4 <= n && ti >= 0) {
+                        if (n >= 5 && a + 6 <= n && ti >= 0) {
                             P.tail_depth = a;
                             P.tail_bms = (uint32_t)hb.bm_words;
                             hb.bm_words += (uint64_t)c->cnt[order[n - 2]] / 32 + 1;

@@ -149,13 +149,13 @@ def test_emulated_factored_tail(emu, port):
     tail: one sum per shallow node, corrected per node by inclusion-exclusion
     over the embedded vertices) against the oracle, with the tail on (default)
     and off (bitmap_min = -1)."""
-    g = smx_generate(600, 2400, 7)
-    off, nb, lab = g.csr()
-    dg = emu.graph(off, nb, lab)
-    path = os.path.join(TMP, "g600_2400_7.txt")
-    g.save(path)
-    gp = port.load_graph(path)
-    for k, seed in [(8, 1055), (7, 1110), (6, 1157)]:
+    for gn, gm, gs, k, seed in [(600, 2400, 7, 8, 1055), (900, 4000, 5, 7, 1046), (600, 2400, 7, 7, 1110)]:
+        g = smx_generate(gn, gm, gs)
+        off, nb, lab = g.csr()
+        dg = emu.graph(off, nb, lab)
+        path = os.path.join(TMP, f"g{gn}_{gm}_{gs}.txt")
+        g.save(path)
+        gp = port.load_graph(path)
         q = smx_query(g, k, seed)
         qpath = os.path.join(TMP, f"tail_q{seed}.txt")
         q.save(qpath)
