@@ -1382,6 +1382,9 @@ __device__ uint32_t compute_ops(const QPlan& P, uint32_t dd, uint32_t v, uint32_
     const uint64_t o0 = __ldg(P.off + v);
     const uint32_t dv = (uint32_t)(__ldg(P.off + v + 1) - o0);
     const uint32_t* nv = P.adj + o0;
+    // v a hub: a short parent list is tested against v by adjacency (hub
+    // matrix or the shorter row) instead of searching v's long row
+    const uint32_t hv = (D.nops && P.hub_words) ? __ldg(P.hub_id + v) : kInvalid;
     for (uint32_t k = 0; k < D.nops; ++k) {
         const uint32_t id = D.ops_begin + k;
         const OpInfo O = P.op[id];
@@ -1395,8 +1398,26 @@ __device__ uint32_t compute_ops(const QPlan& P, uint32_t dd, uint32_t v, uint32_
             uint32_t* out = scr + O.scr_off;
             C.isect++;
             C.bytes += 4ull * (par.len + dv);
-            if (par.len <= dv) len = isect<false>(st, gallop_ratio, par.p, par.len, nv, dv, out);
-            else len = isect<false>(st, gallop_ratio, nv, dv, par.p, par.len, out);
+            if (hv != kInvalid && (uint64_t)par.len * gallop_ratio < dv) {
+                len = 0;
+                for (uint32_t base = 0; base < par.len; base += 32) {
+                    const uint32_t i = base + lane_id();
+                    uint32_t x = 0;
+                    bool hit = false;
+                    if (i < par.len) {
+                        x = par.p[i];
+                        hit = adjacent(P, v, hv, x, __ldg(P.hub_id + x));
+                    }
+                    const uint32_t b = __ballot_sync(kFull, hit);
+                    if (hit) out[len + __popc(b & lanemask_lt())] = x;
+                    len += __popc(b);
+                }
+                __syncwarp();
+            } else if (par.len <= dv) {
+                len = isect<false>(st, gallop_ratio, par.p, par.len, nv, dv, out);
+            } else {
+                len = isect<false>(st, gallop_ratio, nv, dv, par.p, par.len, out);
+            }
             p = out;
         }
         __syncwarp();
