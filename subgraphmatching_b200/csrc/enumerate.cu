@@ -107,6 +107,7 @@ struct QPlan {
     uint32_t leaf_g_off;   // kInvalid unless G is a partial buffer
     uint32_t leaf_gp_off;  // buffer for G without the embedded vertices
     uint32_t leaf_bm;      // 1: G may be marked in the warp's bitmap (indices into C(u_L))
+    uint32_t leaf_gdepth;  // deepest depth G depends on when < n-3 (G may stay marked), else kInvalid
     uint32_t hub_words;    // words per row of the hub adjacency matrix (0: none)
     const uint32_t* hub_id;
     const uint32_t* hub_bits;
@@ -666,6 +667,10 @@ __device__ bool compute_parts(const QPlan& P, uint32_t d, uint32_t* scr, Stage& 
 //          needed only where G is unconstrained);
 //   K0     |G| - #valid pranks (the count when n-2 is not a backward neighbour).
 // Then every candidate of depth n-2 is counted by its own lane (leaf_batch).
+// G longer than this stays marked across depth-(n-2) lists when it can
+#ifndef SMX_LEAF_PERSIST_MIN
+#define SMX_LEAF_PERSIST_MIN 256
+#endif
 struct LeafState {
     uint64_t gptr;
     uint32_t glen;
@@ -676,6 +681,7 @@ struct LeafState {
     uint32_t prank0, prank1;
     uint64_t pmask;    // depths with a valid prank
     uint32_t* bm;      // the warp bitmap while G is marked in it, else null
+    uint32_t persist;  // 1: G (with the embedded vertices) stays marked beyond this depth-(n-2) list
     uint32_t hub;      // 1: G's vertex ids and hub ids are staged after G (shared memory, words 256 / 512)
 };
 
@@ -700,6 +706,10 @@ __device__ __forceinline__ uint32_t lane_count_bitmap(const uint32_t* row, uint3
 // else runs at depth n-2).
 __device__ void leaf_clear(LeafState& S) {
     if (!S.bm) return;
+    if (S.persist) {  // unmarked when its prefix changes
+        S.bm = nullptr;
+        return;
+    }
     const uint32_t* g = reinterpret_cast<const uint32_t*>(S.gptr);
     __syncwarp();
     for (uint32_t i = lane_id(); i < S.glen; i += 32) atomicAnd(S.bm + (g[i] >> 5), ~(1u << (g[i] & 31)));
@@ -708,7 +718,8 @@ __device__ void leaf_clear(LeafState& S) {
 }
 
 __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uint32_t (&slot_idx)[2],
-                             const uint32_t (&slot_vid)[2], LeafState& S, uint32_t* bm, uint32_t bitmap_min) {
+                             const uint32_t (&slot_vid)[2], LeafState& S, uint32_t* bm, uint32_t bitmap_min,
+                             bool& g_live) {
     const uint32_t lane = lane_id();
     const uint32_t L = P.n - 1;
     const DepthInfo& D = P.dep[L];
@@ -747,6 +758,21 @@ __device__ void leaf_prepare(const QPlan& P, uint32_t* scr, Stage& st, const uin
     S.pmask = pm;
     S.k0 = S.glen - __popcll(pm);
     S.hub = 0;
+    S.persist = 0;
+    if (S.inb && S.gany && bm && P.leaf_gdepth != kInvalid && G.len > SMX_LEAF_PERSIST_MIN) {
+        // a long G that depends only on depths above n-3: it stays marked
+        // while they keep their candidates, and the embedded vertices in it
+        // (pmask) are subtracted per candidate instead of being removed
+        if (!g_live) {
+            __syncwarp();
+            for (uint32_t i = lane; i < G.len; i += 32) atomicOr(bm + (G.p[i] >> 5), 1u << (G.p[i] & 31));
+            __syncwarp();
+            g_live = true;
+        }
+        S.bm = bm;
+        S.persist = 1;
+        return;
+    }
     if (S.inb && S.gany) {
         // G minus the embedded vertices, into shared memory when it fits (the
         // stage buffer is idle until depth n-2 is left), else into its buffer;
@@ -1219,6 +1245,17 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
     uint32_t d = 2;
     LeafState leaf;
     leaf.bm = nullptr;
+    leaf.persist = 0;
+    // a long G kept marked across depth-(n-2) lists (see leaf_prepare)
+    bool g_live = false;
+    auto g_drop = [&]() {
+        if (!g_live) return;
+        const Row G = tail_list(P, scr, P.leaf_g_off, P.leaf_g_bn, slot_idx);
+        __syncwarp();
+        for (uint32_t i = lane; i < G.len; i += 32) atomicAnd(bm + (G.p[i] >> 5), ~(1u << (G.p[i] & 31)));
+        __syncwarp();
+        g_live = false;
+    };
     // factored tail: S and G marked in the bitmaps and B valid for the current prefix
     const bool tail = P.tail_depth != kInvalid && bm != nullptr;
     bool tail_live = false;
@@ -1267,7 +1304,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
             SLOT_SET(len, dd, 0u);
             return;
         }
-        if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf, bm, A.bitmap_min);
+        if (dd + 2 == n && r.len) leaf_prepare(P, scr, st, slot_idx, slot_vid, leaf, bm, A.bitmap_min, g_live);
     };
     open_depth(2);
     uint32_t iter = 0;
@@ -1345,6 +1382,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
         const uint32_t c = lp[pos];
         const uint32_t v = __ldg(P.dep[d].cand + c);
         if (tail && d <= P.tail_depth) tail_drop();  // S and G change with this depth
+        if (d <= P.leaf_gdepth) g_drop();             // as does a persistent G
         SLOT_SET(idx, d, c);
         SLOT_SET(vid, d, v);
         C.nodes++;
@@ -1354,6 +1392,7 @@ __device__ void run_table_task(const EnumArgs& A, const QPlan& P, uint64_t t, ui
     }
     leaf_clear(leaf);  // a stop can leave depth n-2 early
     tail_drop();
+    g_drop();
 #undef idx0
 #undef idx1
 #undef vid0
@@ -1785,6 +1824,7 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
     }
     P.leaf_inb = 0;
     P.leaf_bm = 0;
+    P.leaf_gdepth = kInvalid;
     P.tail_depth = kInvalid;
     P.tail_bms = 0;
     P.leaf_g_bn = P.leaf_g_off = P.leaf_gp_off = kInvalid;
@@ -1830,7 +1870,11 @@ int build_host_plan(const smx_graph* g, const HostQuery& q, const smx_cand* c, c
                         for (uint32_t p : bnd[n - 2]) a = std::max(a, p);
                         for (uint32_t j = 0; j < jmax; ++j) a = std::max(a, bnd[t][j]);
                         const int ti = c->tab_index[order[t]][order[n - 2]];
+                        uint32_t ag = 0;
+                        for (uint32_t j = 0; j < jmax; ++j) ag = std::max(ag, bnd[t][j]);
+                        if (ag + 4 <= n) P.leaf_gdepth = ag;
                         if (n >= 5 && a + 6 <= n && ti >= 0) {
+                            P.leaf_gdepth = kInvalid;  // the tail keeps its own marks
                             P.tail_depth = a;
                             P.tail_bms = (uint32_t)hb.bm_words;
                             hb.bm_words += (uint64_t)c->cnt[order[n - 2]] / 32 + 1;
